@@ -1,0 +1,127 @@
+/* smili_b200: C ABI of the B200 static-imaging solver (libsmili_b200.so).
+ *
+ * Replaces the native core that SMILI reaches through its f2py module
+ * `fortlib` (built from src/fortlib/*.f90 by src/fortlib/makefile.in:135-136):
+ * the objective/gradient evaluation calc_cost (src/fortlib/fftim2d.f90:387)
+ * and the L-BFGS-B driver fftim2d.imaging (src/fortlib/fftim2d.f90:11-382),
+ * including the FINUFFT transforms it calls (src/wrapfinufft/wrapfinufft.f90).
+ *
+ * All entry points return SMILI_OK (0) or a negative error code; the text of
+ * the last error of the calling thread is available from smili_last_error().
+ * Device memory is allocated and owned by the library; callers pass host
+ * pointers only.  Arrays use the Fortran layouts of the reference: image
+ * vectors of Npix pixels with 1-based xidx/yidx, uvidxcp as (3,Ncp) and
+ * uvidxca as (4,Nca) column-major (the indices of one datum contiguous).
+ */
+#ifndef SMILI_B200_H
+#define SMILI_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMILI_OK 0
+#define SMILI_ERR_ARG (-1)         /* invalid size, index or option */
+#define SMILI_ERR_DATA (-2)        /* non-finite value or non-positive variance */
+#define SMILI_ERR_CUDA (-3)        /* CUDA runtime failure */
+#define SMILI_ERR_NODEV (-4)       /* no usable CUDA device */
+#define SMILI_ERR_TIMEOUT (-5)     /* a device-side wait gave up (solve aborted) */
+#define SMILI_ERR_UNSUPPORTED (-6) /* e.g. L-BFGS-B memory m > 6 */
+
+/* Solver task codes reported in smili_solve_info.task */
+#define SMILI_TASK_CONV 3      /* CONVERGENCE: pgtol or factr test */
+#define SMILI_TASK_ABNORMAL 4  /* ABNORMAL_TERMINATION_IN_LNSRCH */
+#define SMILI_TASK_STOP 5      /* STOP: TOTAL ITERATION NUMBER EXCEEDS LIMIT */
+#define SMILI_TASK_ERROR 6
+
+/* The arguments of fortlib.fftim2d.imaging / calc_cost
+ * (src/fortlib/fftim2d.f90:11-34, smili/imaging/lbfgs.py:492-564). */
+typedef struct {
+  int npix, nx, ny;
+  const double* iin;
+  const int* xidx;
+  const int* yidx;
+  double nxref, nyref;
+  int nuv;
+  const double* u;
+  const double* v;
+  double l1_l;  const double* l1_wgt;  int l1_nwgt;
+  double tv_l;  const double* tv_wgt;  int tv_nwgt;
+  double tsv_l; const double* tsv_wgt; int tsv_nwgt;
+  double kl_l;  const double* kl_wgt;  int kl_nwgt;
+  double gs_l;  const double* gs_wgt;  int gs_nwgt;
+  double tfd_l, tfd_tgtfd;
+  double cen_l, cen_alpha;
+  double sm_l, sm_maj, sm_min, sm_phi;
+  int isfcv, nfcv; const int* uvidxfcv; const double* vfcvr; const double* vfcvi; const double* varfcv; double wfcv;
+  int isamp, namp; const int* uvidxamp; const double* vamp; const double* varamp; double wamp;
+  int iscp, ncp;   const int* uvidxcp;  const double* cp;   const double* varcp;  double wcp;
+  int isca, nca;   const int* uvidxca;  const double* ca;   const double* varca;  double wca;
+  double inormfactr;
+} smili_imaging_args;
+
+/* Options that have no counterpart in the reference's signature. */
+typedef struct {
+  int precision;        /* 64 (default, FP64 throughout) or 32 (FP32 transforms,
+                           compensated FP32 chi-square sums, FP64 optimiser) */
+  double nufft_eps;     /* NUFFT tolerance; 0 -> 1e-6 (the reference's ffteps) */
+  int ctas_per_problem; /* 0 -> automatic */
+  int device;           /* CUDA device ordinal */
+  void* stream;         /* cudaStream_t, NULL -> the library's own stream */
+} smili_options;
+
+typedef struct {
+  int task;   /* SMILI_TASK_* */
+  int niter;  /* L-BFGS-B iterations completed (isave(30)) */
+  int nfg;    /* function/gradient evaluations, including the final summary */
+  int error;  /* nonzero when the solve was aborted */
+} smili_solve_info;
+
+/* terms[15] = chisq, chisqfcv, chisqamp, chisqcp, chisqca, reg, l1_cost,
+ * tv_cost, tsv_cost, kl_cost, gs_cost, tfd_cost, cen_cost, sm_cost, cost
+ * (the intent(out) scalars of fftim2d.imaging, fftim2d.f90:29-32). */
+
+/* fortlib.fftim2d.imaging (fftim2d.f90:11-382): L-BFGS-B with m, factr,
+ * pgtol from smili/imaging/lbfgs.py:34-38, stopped after niter+1 iterations
+ * like fftim2d.f90:324.  Writes Iout[npix] and the final cost terms. */
+int smili_fftim2d_imaging(const smili_imaging_args* a, int niter, int nonneg, int nprint, int m,
+                          double factr, double pgtol, const smili_options* opt, double* iout,
+                          double* terms, smili_solve_info* info);
+
+/* calc_cost (fftim2d.f90:387-607): cost terms and gradient at image x. */
+int smili_calc_cost(const smili_imaging_args* a, const double* x, const smili_options* opt,
+                    double* terms, double* grad);
+
+/* Batched solves: many independent problems (different image sizes, data and
+ * weights) in one persistent launch.  No reference counterpart: the reference
+ * solves one problem per call of fftim2d.imaging. */
+typedef struct smili_batch smili_batch;
+int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const int* niter,
+                       int nonneg, int m, double factr, double pgtol, const smili_options* opt,
+                       smili_batch** out);
+/* Solve (or, with fg_only != 0, evaluate calc_cost once) every problem on the
+ * device; kernel_ms (optional) receives the device time of the launch. */
+int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms);
+int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double* grad,
+                      smili_solve_info* info);
+/* Cost recorded at each completed iteration of problem p (NaN where absent). */
+int smili_batch_trace(smili_batch* b, int p, double* trace, int len);
+void smili_batch_destroy(smili_batch* b);
+
+/* NUFFTs of the imaging path with the reference's conventions (sign "+",
+ * modes -N/2..(N-1)/2 at pixels 1..N): fortlib.fftlib.nufft_fwd_real
+ * (type 2, fftlib.f90:86-100) and nufft_adj_real1d (type 1, real part,
+ * fftlib.f90:118-133).  u, v already multiplied by 2*pi*dx, 2*pi*dy. */
+int smili_nufft_fwd_real(int nuv, const double* u, const double* v, int nx, int ny,
+                         const double* img, const smili_options* opt, double* vreal,
+                         double* vimag);
+int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const double* vreal,
+                           const double* vimag, int nx, int ny, const smili_options* opt,
+                           double* img);
+
+const char* smili_last_error(void);
+int smili_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

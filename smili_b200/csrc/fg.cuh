@@ -1,0 +1,547 @@
+// One function/gradient evaluation of the static-imaging objective, split into
+// stages that the CTAs of a group share (a group barrier separates stages).
+//
+// Replaces calc_cost (src/fortlib/fftim2d.f90:387-607) =
+//   calc_chisq (src/fortlib/fftlib.f90:250-382):
+//     I1d_I2d_fwd + FINUFFT type 2 (wrapfinufft.f90:94-128)   -> stages F1-F3
+//     calc_chisq_fcv/amp/ca/cp (fftlib.f90:384-655)           -> stage F4
+//     NUFFT_adj_resid: 2 x FINUFFT type 1 (fftlib.f90:152-174) -> stages F5-F7
+//       (one type-1 of c = Vresre - i Vresim: Re T1(c) = Re T1(Vresre) + Im T1(Vresim))
+//   + calc_cost_reg (src/fortlib/image.f90:12-200)             -> stage F8
+//
+// NUFFT (exponential-of-semicircle kernel, upsampling 2) restricted to the
+// "band" of fine-grid cells that the uv points touch: the type-2 row pass
+// keeps only band columns and the column pass only runs on band columns; the
+// type-1 passes run only on band rows.  Fine-grid coordinates xi = u n / 2pi
+// are precomputed at set-up.
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+template <typename R>
+__device__ __forceinline__ R es_kernel(R z, R beta) {
+  const R s = (R)1 - z * z;
+  return s > (R)0 ? exp(beta * (sqrt(s) - (R)1)) : (R)0;
+}
+
+__device__ __forceinline__ int imod(int a, int n) {
+  int r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ double smabs(double x) { return sqrt(x * x + 1e-10); }
+
+// rows (sequences) per CTA pass for an FFT of length n
+__device__ __forceinline__ int fft_batch(int n) {
+  int s = (SMILI_THREADS * 8) / n;
+  return s < 1 ? 1 : s;
+}
+
+// Working context of one problem inside a kernel
+template <typename R>
+struct FgCtx {
+  const ProbDesc* P;
+  char* base;
+  cpx<R>* sbuf;   // shared: 2 * SMEM_CPX complex values
+  cpx<R>* swork;
+  int smem_cpx;   // capacity of each of the two buffers (complex elements)
+};
+
+// Running compensated sum (TwoSum) used for the chi-square terms
+struct KSum {
+  double s, c;
+  __device__ void add(double v) {
+    const double t = s + v;
+    const double bp = t - s;
+    c += (s - (t - bp)) + (v - bp);
+    s = t;
+  }
+  __device__ double value() const { return s + c; }
+};
+struct KSumF {
+  float s, c;
+  __device__ void add(float v) {
+    const float t = s + v;
+    const float bp = t - s;
+    c += (s - (t - bp)) + (v - bp);
+    s = t;
+  }
+  __device__ double value() const { return (double)s + (double)c; }
+};
+
+// ---------------------------------------------------------------------------
+// F1: type-2 row pass.  Deconvolved image rows -> band columns of the
+// row-transformed fine grid (tmpA[iy][b], b < b1n).  Also zeroes bandC.
+// Optionally accumulates image moments for the global regularizers.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
+  const ProbDesc& P = *c.P;
+  const double* x = at<double>(c.base, P.o_x);
+  const int* inv = at<int>(c.base, P.o_inv);
+  const double* dc1 = at<double>(c.base, P.o_dc1);
+  const double* dc2 = at<double>(c.base, P.o_dc2);
+  const cpx<R>* tw1 = at<cpx<R>>(c.base, P.o_tw1);
+  cpx<R>* tmpA = at<cpx<R>>(c.base, P.o_tmpA);
+  cpx<R>* bandC = at<cpx<R>>(c.base, P.o_bandC);
+  const int n1 = P.nf1, nx = P.nx, ny = P.ny;
+  const FftPlan pl = make_plan(n1);
+  const int S = min(fft_batch(n1), c.smem_cpx / n1);
+  for (int i = g.rank * SMILI_THREADS + threadIdx.x; i < P.b2n * P.b1n; i += g.G * SMILI_THREADS)
+    bandC[i] = cmk<R>(0, 0);
+  const bool need_mom = P.has_tfd || P.has_cen || P.has_sm;
+  for (int row0 = g.rank * S; row0 < ny; row0 += g.G * S) {
+    const int rows = min(S, ny - row0);
+    for (int i = threadIdx.x; i < rows * n1; i += blockDim.x) c.sbuf[i] = cmk<R>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * nx; i += blockDim.x) {
+      const int s = i / nx, ix = i - s * nx, iy = row0 + s;
+      const int pv = inv[iy * nx + ix];
+      const double val = pv >= 0 ? x[pv] : 0.0;
+      c.sbuf[s * n1 + imod(ix - nx / 2, n1)] = cmk<R>((R)(val * dc1[ix] * dc2[iy]), (R)0);
+      if (need_mom && pv >= 0) {
+        const double fx = ix + 1, fy = iy + 1;  // 1-based pixel numbers as the reference
+        mom[0] += val;
+        mom[1] += fabs(val);
+        mom[2] += val * fx;
+        mom[3] += val * fy;
+        mom[4] += val * fx * fx;
+        mom[5] += val * fy * fy;
+        mom[6] += val * fx * fy;
+        if (P.has_cen) {
+          const double Ip = fabs(P.cen_alpha - 1) < 1e-10 ? smabs(val) : pow(smabs(val), P.cen_alpha);
+          mom[7] += Ip * (fx - P.nxref);
+          mom[8] += Ip * (fy - P.nyref);
+          mom[9] += Ip;
+        }
+      }
+    }
+    __syncthreads();
+    const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, rows, tw1);
+    for (int i = threadIdx.x; i < rows * P.b1n; i += blockDim.x) {
+      const int s = i / P.b1n, b = i - s * P.b1n;
+      tmpA[(size_t)(row0 + s) * P.b1n + b] = out[s * n1 + imod(P.b1s + b, n1)];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// F2: type-2 column pass over band columns -> bandA[b2][b1]
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void fg_t2_cols(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* tw2 = at<cpx<R>>(c.base, P.o_tw2);
+  const cpx<R>* tmpA = at<cpx<R>>(c.base, P.o_tmpA);
+  cpx<R>* bandA = at<cpx<R>>(c.base, P.o_bandA);
+  const int n2 = P.nf2, ny = P.ny, b1n = P.b1n;
+  const FftPlan pl = make_plan(n2);
+  const int S = min(fft_batch(n2), c.smem_cpx / n2);
+  for (int b0 = g.rank * S; b0 < b1n; b0 += g.G * S) {
+    const int cols = min(S, b1n - b0);
+    for (int i = threadIdx.x; i < cols * n2; i += blockDim.x) c.sbuf[i] = cmk<R>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
+      const int iy = i / cols, s = i - iy * cols;
+      c.sbuf[s * n2 + imod(iy - ny / 2, n2)] = tmpA[(size_t)iy * b1n + b0 + s];
+    }
+    __syncthreads();
+    const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, cols, tw2);
+    for (int i = threadIdx.x; i < cols * P.b2n; i += blockDim.x) {
+      const int b2 = i / cols, s = i - b2 * cols;
+      bandA[(size_t)b2 * b1n + b0 + s] = out[s * n2 + imod(P.b2s + b2, n2)];
+    }
+    __syncthreads();
+  }
+}
+
+// kernel taps of one point: first cell index and the w weights per axis
+template <typename R>
+__device__ __forceinline__ void taps(R xi, int w, R beta, int& l0, R* k) {
+  const R half = (R)0.5 * (R)w;
+  l0 = (int)ceil(xi - half);
+  const R inv = (R)1 / half;
+  for (int a = 0; a < w; ++a) k[a] = es_kernel(((R)(l0 + a) - xi) * inv, beta);
+}
+
+// ---------------------------------------------------------------------------
+// F3: type-2 interpolation, V_j = sum psi psi bandA
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const R* xu = at<R>(c.base, P.o_u);
+  const R* xv = at<R>(c.base, P.o_v);
+  const cpx<R>* bandA = at<cpx<R>>(c.base, P.o_bandA);
+  cpx<R>* V = at<cpx<R>>(c.base, P.o_V);
+  const int w = P.w;
+  const R beta = (R)P.beta;
+  for (int j = g.rank * SMILI_THREADS + threadIdx.x; j < P.nuv; j += g.G * SMILI_THREADS) {
+    int l1, l2;
+    R k1[SMILI_MAXW], k2[SMILI_MAXW];
+    taps(xu[j], w, beta, l1, k1);
+    taps(xv[j], w, beta, l2, k2);
+    const int c1 = imod(l1 - P.b1s, P.nf1), c2 = imod(l2 - P.b2s, P.nf2);
+    R ar = 0, ai = 0;
+    for (int b = 0; b < w; ++b) {
+      int rw = c2 + b;  // wraps only when the band spans the whole fine grid
+      if (rw >= P.nf2) rw -= P.nf2;
+      const cpx<R>* row = bandA + (size_t)rw * P.b1n;
+      R rr = 0, ri = 0;
+      for (int a = 0; a < w; ++a) {
+        int cl = c1 + a;
+        if (cl >= P.nf1) cl -= P.nf1;
+        const cpx<R> q = row[cl];
+        rr += k1[a] * q.x;
+        ri += k1[a] * q.y;
+      }
+      ar += k2[b] * rr;
+      ai += k2[b] * ri;
+    }
+    V[j] = cmk(ar, ai);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// F4: chi-square terms and their derivatives per contribution slot.
+// chi[0..3] = fcv, amp, cp, ca (weighted by the normalised data weights).
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* V = at<cpx<R>>(c.base, P.o_V);
+  const R* dre = at<R>(c.base, P.o_dre);
+  const R* dim = at<R>(c.base, P.o_dim);
+  const R* dvar = at<R>(c.base, P.o_dvar);
+  const int* didx = at<int>(c.base, P.o_didx);
+  const signed char* dsgn = at<signed char>(c.base, P.o_dsgn);
+  cpx<R>* contrib = at<cpx<R>>(c.base, P.o_contrib);
+  typedef typename std::conditional<sizeof(R) == 8, KSum, KSumF>::type Acc;
+  Acc acc[4];
+  for (int q = 0; q < 4; ++q) acc[q].s = acc[q].c = 0;
+  const int e_amp = P.nfcv, e_cp = e_amp + P.namp, e_ca = e_cp + P.ncp, e_end = e_ca + P.nca;
+  const int s_amp = P.nfcv, s_cp = s_amp + P.namp, s_ca = s_cp + 3 * P.ncp;
+  const R wf = (R)P.wfcv, wa = (R)P.wamp, wc = (R)P.wcp, wq = (R)P.wca;
+  for (int i = g.rank * SMILI_THREADS + threadIdx.x; i < e_end; i += g.G * SMILI_THREADS) {
+    const R var = dvar[i];
+    if (i < e_amp) {  // complex visibilities (fftlib.f90:384-439)
+      const int slot = i;
+      const int k = didx[slot];
+      const R sg = (R)dsgn[slot];
+      const cpx<R> Vk = V[k];
+      const R rr = dre[i] - Vk.x, ri = dim[i] - sg * Vk.y;
+      acc[0].add(((rr * rr + ri * ri) / var) * wf);
+      const R factor = (R)-2 / var * wf;
+      contrib[slot] = cmk(factor * rr, factor * ri * sg);
+    } else if (i < e_cp) {  // amplitudes (fftlib.f90:442-493)
+      const int slot = s_amp + (i - e_amp);
+      const cpx<R> Vk = V[didx[slot]];
+      const R model = sqrt(Vk.x * Vk.x + Vk.y * Vk.y);
+      const R resid = dre[i] - model;
+      acc[1].add((resid * resid / var) * wa);
+      const R factor = (R)-2 * resid / var / model * wa;
+      contrib[slot] = cmk(factor * Vk.x, factor * Vk.y);
+    } else if (i < e_ca) {  // closure phases (fftlib.f90:576-655)
+      const int slot = s_cp + 3 * (i - e_cp);
+      cpx<R> Vq[3];
+      R a2[3], sg[3];
+      R model = 0;
+      for (int q = 0; q < 3; ++q) {
+        Vq[q] = V[didx[slot + q]];
+        sg[q] = (R)dsgn[slot + q];
+        a2[q] = Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y;
+        model = atan2(Vq[q].y, Vq[q].x) * sg[q] + model;
+      }
+      const R resid = dre[i] - model;
+      R sr, cr;
+      if (sizeof(R) == 8) {
+        double s_, c_;
+        sincos((double)resid, &s_, &c_);
+        sr = (R)s_;
+        cr = (R)c_;
+      } else {
+        float s_, c_;
+        sincosf((float)resid, &s_, &c_);
+        sr = (R)s_;
+        cr = (R)c_;
+      }
+      acc[2].add(((R)2 * ((R)1 - cr) / var) * wc);
+      const R factor = (R)-2 * sr / var * wc;
+      for (int q = 0; q < 3; ++q)
+        contrib[slot + q] = cmk(-factor / a2[q] * Vq[q].y * sg[q], factor / a2[q] * Vq[q].x * sg[q]);
+    } else {  // log closure amplitudes (fftlib.f90:496-573)
+      const int slot = s_ca + 4 * (i - e_ca);
+      cpx<R> Vq[4];
+      R a[4];
+      for (int q = 0; q < 4; ++q) {
+        Vq[q] = V[didx[slot + q]];
+        a[q] = sqrt(Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y);
+      }
+      const R model = log(a[0]) + log(a[1]) - log(a[2]) - log(a[3]);
+      const R resid = dre[i] - model;
+      acc[3].add((resid * resid / var) * wq);
+      const R factor = (R)-2 * resid / var * wq;
+      for (int q = 0; q < 4; ++q) {
+        const R f = (q < 2 ? factor : -factor) / (a[q] * a[q]);
+        contrib[slot + q] = cmk(f * Vq[q].x, f * Vq[q].y);
+      }
+    }
+  }
+  for (int q = 0; q < 4; ++q) chi[q] += acc[q].value();
+}
+
+// ---------------------------------------------------------------------------
+// F5: gather the derivative slots of each uv point (CSR) and spread
+// c_j = Vresre_j - i Vresim_j onto bandC.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void atomic_add_r(double* p, double v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atomic_add_r(float* p, float v) { atomicAdd(p, v); }
+
+template <typename R>
+__device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const R* xu = at<R>(c.base, P.o_u);
+  const R* xv = at<R>(c.base, P.o_v);
+  const int* off = at<int>(c.base, P.o_csr_off);
+  const int* ent = at<int>(c.base, P.o_csr_ent);
+  const cpx<R>* contrib = at<cpx<R>>(c.base, P.o_contrib);
+  R* band = at<R>(c.base, P.o_bandC);
+  const int w = P.w;
+  const R beta = (R)P.beta;
+  for (int j = g.rank * SMILI_THREADS + threadIdx.x; j < P.nuv; j += g.G * SMILI_THREADS) {
+    R cre = 0, cim = 0;
+    for (int e = off[j]; e < off[j + 1]; ++e) {
+      const cpx<R> q = contrib[ent[e]];
+      cre += q.x;
+      cim += q.y;
+    }
+    cim = -cim;  // c = Vresre - i Vresim
+    int l1, l2;
+    R k1[SMILI_MAXW], k2[SMILI_MAXW];
+    taps(xu[j], w, beta, l1, k1);
+    taps(xv[j], w, beta, l2, k2);
+    const int c1 = imod(l1 - P.b1s, P.nf1), c2 = imod(l2 - P.b2s, P.nf2);
+    for (int b = 0; b < w; ++b) {
+      int rw = c2 + b;
+      if (rw >= P.nf2) rw -= P.nf2;
+      R* row = band + 2 * (size_t)rw * P.b1n;
+      const R wr = k2[b] * cre, wi = k2[b] * cim;
+      for (int a = 0; a < w; ++a) {
+        int cl = c1 + a;
+        if (cl >= P.nf1) cl -= P.nf1;
+        atomic_add_r(row + 2 * cl, k1[a] * wr);
+        atomic_add_r(row + 2 * cl + 1, k1[a] * wi);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// F6: type-1 row pass over band rows -> tmpC[b2][ix] (modes along axis 1)
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void fg_t1_rows(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* tw1 = at<cpx<R>>(c.base, P.o_tw1);
+  const cpx<R>* bandC = at<cpx<R>>(c.base, P.o_bandC);
+  cpx<R>* tmpC = at<cpx<R>>(c.base, P.o_tmpC);
+  const int n1 = P.nf1, nx = P.nx, b1n = P.b1n;
+  const FftPlan pl = make_plan(n1);
+  const int S = min(fft_batch(n1), c.smem_cpx / n1);
+  for (int r0 = g.rank * S; r0 < P.b2n; r0 += g.G * S) {
+    const int rows = min(S, P.b2n - r0);
+    for (int i = threadIdx.x; i < rows * n1; i += blockDim.x) c.sbuf[i] = cmk<R>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < rows * b1n; i += blockDim.x) {
+      const int s = i / b1n, b = i - s * b1n;
+      c.sbuf[s * n1 + imod(P.b1s + b, n1)] = bandC[(size_t)(r0 + s) * b1n + b];
+    }
+    __syncthreads();
+    const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, rows, tw1);
+    for (int i = threadIdx.x; i < rows * nx; i += blockDim.x) {
+      const int s = i / nx, ix = i - s * nx;
+      tmpC[(size_t)(r0 + s) * nx + ix] = out[s * n1 + imod(ix - nx / 2, n1)];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// F7: type-1 column pass -> gchi[iy][ix] = Re(F) * dc1 * dc2
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ void fg_t1_cols(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* tw2 = at<cpx<R>>(c.base, P.o_tw2);
+  const cpx<R>* tmpC = at<cpx<R>>(c.base, P.o_tmpC);
+  const double* dc1 = at<double>(c.base, P.o_dc1);
+  const double* dc2 = at<double>(c.base, P.o_dc2);
+  double* gchi = at<double>(c.base, P.o_gchi);
+  const int n2 = P.nf2, nx = P.nx, ny = P.ny;
+  const FftPlan pl = make_plan(n2);
+  const int S = min(fft_batch(n2), c.smem_cpx / n2);
+  for (int x0 = g.rank * S; x0 < nx; x0 += g.G * S) {
+    const int cols = min(S, nx - x0);
+    for (int i = threadIdx.x; i < cols * n2; i += blockDim.x) c.sbuf[i] = cmk<R>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cols * P.b2n; i += blockDim.x) {
+      const int b2 = i / cols, s = i - b2 * cols;
+      c.sbuf[s * n2 + imod(P.b2s + b2, n2)] = tmpC[(size_t)b2 * nx + x0 + s];
+    }
+    __syncthreads();
+    const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, cols, tw2);
+    for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
+      const int iy = i / cols, s = i - iy * cols, ix = x0 + s;
+      gchi[(size_t)iy * nx + ix] = (double)out[s * n2 + imod(iy - ny / 2, n2)].x * dc1[ix] * dc2[iy];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// F8: regularizers + gradient assembly g = gradchisq + gradreg.
+// reg[0..7] = l1, tv, tsv, kl, gs, tfd, cen, sm.  Also returns g.d and the
+// projected-gradient infinity norm used by the optimiser.
+// mom: reduced image moments from F1 (only when tfd/cen/sm are active).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double px(const double* x, const int* inv, int nx, int ny, int ix, int iy) {
+  if (ix < 0 || iy < 0 || ix >= nx || iy >= ny) return 0.0;
+  const int p = inv[iy * nx + ix];
+  return p >= 0 ? x[p] : 0.0;
+}
+
+__device__ double tv_grade_px(const double* x, const int* inv, int nx, int ny, int i1, int j1) {
+  // image.f90:512-612 with 0-based (i1, j1); reproduces the gradient reset
+  double gr = 0.0;
+  const double I11 = px(x, inv, nx, ny, i1, j1);
+  double dIx = (i1 + 1 >= nx) ? 0.0 : px(x, inv, nx, ny, i1 + 1, j1) - I11;
+  double dIy = (j1 + 1 >= ny) ? 0.0 : px(x, inv, nx, ny, i1, j1 + 1) - I11;
+  double e = sqrt(dIx * dIx + dIy * dIy);
+  if (e > 1e-10) gr -= (dIx + dIy) / e;
+  if (i1 - 1 >= 0) {
+    const double I01 = px(x, inv, nx, ny, i1 - 1, j1);
+    dIx = I11 - I01;
+    dIy = (j1 + 1 >= ny) ? 0.0 : px(x, inv, nx, ny, i1 - 1, j1 + 1) - I01;
+    e = sqrt(dIx * dIx + dIy * dIy);
+    if (e > 1e-10) gr += dIx / e;
+    else gr = 0.0;
+  }
+  if (j1 - 1 >= 0) {
+    const double I10 = px(x, inv, nx, ny, i1, j1 - 1);
+    dIy = I11 - I10;
+    dIx = (i1 + 1 >= nx) ? 0.0 : px(x, inv, nx, ny, i1 + 1, j1 - 1) - I10;
+    e = sqrt(dIx * dIx + dIy * dIy);
+    if (e > 1e-10) gr += dIy / e;
+    else gr = 0.0;
+  }
+  return gr;
+}
+
+struct RegMoments {
+  double Isum_abs, xcen, ycen, Sg[3], mom[2], Sp[3];
+  double tfd_resid;
+  double cen_sx, cen_sy, cen_sI, cen_cost;
+};
+
+__device__ void reg_moments(const ProbDesc& P, const double (&m)[10], RegMoments& r) {
+  r.tfd_resid = m[0] - P.tfd_tgtfd;
+  r.Isum_abs = m[1];
+  r.xcen = m[2] / m[1];
+  r.ycen = m[3] / m[1];
+  const double S = m[0];
+  // second moments about the |I|-normalised centroid from raw moments
+  r.Sg[0] = (m[4] - 2 * r.xcen * m[2] + r.xcen * r.xcen * S) / r.Isum_abs;
+  r.Sg[1] = (m[5] - 2 * r.ycen * m[3] + r.ycen * r.ycen * S) / r.Isum_abs;
+  r.Sg[2] = (m[6] - r.xcen * m[3] - r.ycen * m[2] + r.xcen * r.ycen * S) / r.Isum_abs;
+  r.mom[0] = m[2] - r.xcen * S;
+  r.mom[1] = m[3] - r.ycen * S;
+  const double cp = cos(P.sm_phi), sp = sin(P.sm_phi);
+  r.Sp[0] = P.sm_min * cp * cp + P.sm_maj * sp * sp;
+  r.Sp[1] = P.sm_min * sp * sp + P.sm_maj * cp * cp;
+  r.Sp[2] = (P.sm_maj - P.sm_min) * sp * cp;
+  r.cen_sI = m[9] + 1e-10;
+  r.cen_sx = m[7] / r.cen_sI;
+  r.cen_sy = m[8] / r.cen_sI;
+  r.cen_cost = sqrt(r.cen_sx * r.cen_sx + r.cen_sy * r.cen_sy + 1e-10);
+}
+
+__device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, const RegMoments& rm,
+                            int lo, int hi, double (&reg)[8], double& gd, double& sbg) {
+  const double* x = at<double>(base, P.o_x);
+  const int* inv = at<int>(base, P.o_inv);
+  const int* xi = at<int>(base, P.o_xidx);
+  const int* yi = at<int>(base, P.o_yidx);
+  const double* gchi = at<double>(base, P.o_gchi);
+  const double* d = at<double>(base, P.o_d);
+  double* gout = at<double>(base, P.o_g);
+  const double* l1w = P.has_l1 ? at<double>(base, P.o_l1w) : nullptr;
+  const double* tvw = P.has_tv ? at<double>(base, P.o_tvw) : nullptr;
+  const double* tsvw = P.has_tsv ? at<double>(base, P.o_tsvw) : nullptr;
+  const double* klw = P.has_kl ? at<double>(base, P.o_klw) : nullptr;
+  const double* gsw = P.has_gs ? at<double>(base, P.o_gsw) : nullptr;
+  const int nx = P.nx, ny = P.ny;
+  for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+    const int ix = xi[p], iy = yi[p];
+    const double I = x[p];
+    double gr = 0.0;
+    if (P.has_tfd) gr += P.tfd_l * 2 * rm.tfd_resid;
+    if (P.has_cen) {
+      const double dix = (ix + 1) - P.nxref, diy = (iy + 1) - P.nyref;
+      const double gIp = fabs(P.cen_alpha - 1) < 1e-10
+                             ? I / smabs(I)
+                             : I / smabs(I) * P.cen_alpha * pow(smabs(I), P.cen_alpha - 1);
+      gr += P.cen_l * ((rm.cen_sx * (dix - rm.cen_sx) + rm.cen_sy * (diy - rm.cen_sy)) / rm.cen_sI /
+                       rm.cen_cost * gIp);
+    }
+    if (P.has_l1) {
+      const double a = smabs(I);
+      reg[0] += P.l1_l * l1w[p] * a;
+      gr += P.l1_l * l1w[p] * (I / a);
+    }
+    if (P.has_kl) {
+      const double a = smabs(I), pr = klw[p];
+      reg[3] += P.kl_l * (a * log(a / pr) + pr / 2.718281828459045235);
+      gr += P.kl_l * (I / a) * (log(a / pr) + 1);
+    }
+    if (P.has_gs) {
+      const double a = smabs(I), pr = gsw[p];
+      reg[4] += P.gs_l * (a * (log(a / pr) - 1) + pr);
+      gr += P.gs_l * (I / a) * log(a / pr);
+    }
+    if (P.has_tv || P.has_tsv) {
+      const double dIx = (ix + 1 >= nx) ? 0.0 : px(x, inv, nx, ny, ix + 1, iy) - I;
+      const double dIy = (iy + 1 >= ny) ? 0.0 : px(x, inv, nx, ny, ix, iy + 1) - I;
+      if (P.has_tv) {
+        reg[1] += P.tv_l * tvw[p] * sqrt(dIx * dIx + dIy * dIy);
+        gr += P.tv_l * tvw[p] * tv_grade_px(x, inv, nx, ny, ix, iy);
+      }
+      if (P.has_tsv) {
+        reg[2] += P.tsv_l * tsvw[p] * (dIx * dIx + dIy * dIy);
+        double gt = 0.0;
+        if (ix + 1 < nx) gt -= 2 * (px(x, inv, nx, ny, ix + 1, iy) - I);
+        if (iy + 1 < ny) gt -= 2 * (px(x, inv, nx, ny, ix, iy + 1) - I);
+        if (ix - 1 >= 0) gt += 2 * (I - px(x, inv, nx, ny, ix - 1, iy));
+        if (iy - 1 >= 0) gt += 2 * (I - px(x, inv, nx, ny, ix, iy - 1));
+        gr += P.tsv_l * tsvw[p] * gt;
+      }
+    }
+    if (P.has_sm) {
+      const double fx = ix + 1, fy = iy + 1;
+      const double xg = (fx - rm.xcen) / rm.Isum_abs, yg = (fy - rm.ycen) / rm.Isum_abs;
+      const double dx = fx - rm.xcen, dy = fy - rm.ycen;
+      const double s0 = ((dx * dx - 2. * xg * rm.mom[0]) - rm.Sg[0]) / rm.Isum_abs;
+      const double s1 = ((dy * dy - 2. * yg * rm.mom[1]) - rm.Sg[1]) / rm.Isum_abs;
+      const double s2 = (dx * dy - xg * rm.mom[1] - yg * rm.mom[0] - rm.Sg[2]) / rm.Isum_abs;
+      gr += P.sm_l * (2. * (rm.Sg[0] - rm.Sp[0]) * s0 + 2. * (rm.Sg[1] - rm.Sp[1]) * s1 +
+                      4. * (rm.Sg[2] - rm.Sp[2]) * s2);
+    }
+    const double gv = gchi[(size_t)iy * nx + ix] + gr;
+    gout[p] = gv;
+    gd += gv * d[p];
+    // projected gradient (projgr, lbfgsb.f:2942-2990) with lower bound 0
+    double gi = gv;
+    if (P.nonneg && gi >= 0.0) gi = fmin(I, gi);
+    sbg = fmax(sbg, fabs(gi));
+  }
+}

@@ -1,0 +1,87 @@
+// Device-side layout of one imaging problem and of its L-BFGS-B state.
+//
+// Shared by the host packer (host.cu) and the kernels.  Every problem of a
+// batch lives in one device arena; ProbDesc holds the byte offsets of its
+// arrays inside that arena plus the scalars the kernels need.  All offsets
+// are multiples of 256 bytes.
+#pragma once
+#include <stdint.h>
+
+#define SMILI_MAXM 8          // largest L-BFGS-B memory supported on the device
+#define SMILI_MAXW 16         // largest ES kernel width
+#define SMILI_NTERMS 15       // chisq, chisqfcv, chisqamp, chisqcp, chisqca, reg, l1..sm, cost
+#define SMILI_NPART 16        // partial sums produced by one FG evaluation
+
+// data-term kinds in the flattened datum index space
+enum { KIND_FCV = 0, KIND_AMP = 1, KIND_CP = 2, KIND_CA = 3 };
+
+// L-BFGS-B driver states (what the last advance asked for)
+enum {
+  LB_TASK_FG_START = 1,   // evaluate f, g at the projected initial x
+  LB_TASK_FG_LN = 2,      // evaluate f, g at a line-search trial point
+  LB_TASK_CONV = 3,       // converged (pgtol or factr test)
+  LB_TASK_ABNORMAL = 4,   // line search failed with an empty memory
+  LB_TASK_STOP = 5,       // iteration limit reached (iter > niter)
+  LB_TASK_ERROR = 6,      // invalid input or a device-side wait timed out
+  LB_TASK_FG_ONLY = 7     // single evaluation, no optimisation
+};
+
+struct ProbDesc {
+  // sizes
+  int npix, nx, ny, nuv;
+  int nf1, nf2;            // fine grid
+  int w;                   // ES kernel width
+  int b1s, b1n, b2s, b2n;  // band of fine-grid cells touched by the uv points
+  int nfcv, namp, ncp, nca;
+  int nslot;               // contribution slots: nfcv + namp + 3 ncp + 4 nca
+  int ndata;               // nfcv + namp + ncp + nca
+  int nonneg, m, niter, prec64;
+  int has_l1, has_tv, has_tsv, has_kl, has_gs, has_tfd, has_cen, has_sm;
+  int windowed;            // 1 when the pixel set is not the full nx*ny grid
+  int pad0;
+  // scalars
+  double beta;
+  double wfcv, wamp, wcp, wca;       // normalised data weights (w / wtotal)
+  double l1_l, tv_l, tsv_l, kl_l, gs_l, tfd_l, tfd_tgtfd, cen_l, cen_alpha;
+  double sm_l, sm_maj, sm_min, sm_phi;
+  double nxref, nyref;
+  double factr, pgtol;
+  // byte offsets in the arena (0 = absent)
+  int64_t o_x0, o_xidx, o_yidx, o_inv;
+  int64_t o_l1w, o_tvw, o_tsvw, o_klw, o_gsw;
+  int64_t o_dc1, o_dc2, o_tw1, o_tw2;   // deconvolution factors, twiddle tables
+  int64_t o_u, o_v;                     // fine-grid coordinates xi = u n / 2pi (R)
+  int64_t o_dre, o_dim, o_dvar;         // per datum: value(s) and variance (R)
+  int64_t o_didx;                       // per slot: 0-based uv index (sorted order)
+  int64_t o_dsgn;                       // per slot: sign (+1 / -1) as int8
+  int64_t o_csr_off, o_csr_ent;         // uv point -> contribution slots
+  int64_t o_tmpA, o_bandA, o_V, o_contrib, o_bandC, o_tmpC, o_gchi;
+  int64_t o_part;                       // FG partial sums [npart_ctas][SMILI_NPART] (double)
+  // optimiser (double precision)
+  int64_t o_x, o_g, o_z, o_r, o_d, o_t, o_xp, o_ws, o_wy, o_iwh, o_free, o_bkey;
+  int64_t o_cand, o_lred, o_state;
+  int64_t o_trace;                      // cost at each NEW_X (double[niter+2])
+  int64_t o_out;                        // results: terms[15], counters
+};
+
+// Scalar L-BFGS-B state (setulb's isave/dsave/lsave plus the small matrices).
+struct LbState {
+  int task, done, error;
+  int col, head, itail, iupdat, iter, nfgv, ifun, iback, nseg, nskip, nintol, info, iword;
+  int nfree, nact, ileave, nenter;
+  int updatd, wrk, cnstnd, boxed, prjctd;
+  int stage, brackt, csave;
+  int nfg_total;
+  double f, theta, fold, tol, dnorm, gd, gdold, stp, stpmx, sbgnrm, dtd, xstep, epsmch;
+  double ginit, gtest, gx, gy, finit, fx, fy, stx, sty, stmin, stmax, width, width1;
+  double terms[SMILI_NTERMS];
+  double sy[SMILI_MAXM * SMILI_MAXM], ss[SMILI_MAXM * SMILI_MAXM], wt[SMILI_MAXM * SMILI_MAXM];
+  double wn[4 * SMILI_MAXM * SMILI_MAXM], wn1[4 * SMILI_MAXM * SMILI_MAXM];
+  double wa[8 * SMILI_MAXM];
+};
+
+// per-problem results copied back to the host
+struct ProbResult {
+  double terms[SMILI_NTERMS];
+  int task, iter, nfg, error;
+};

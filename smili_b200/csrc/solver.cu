@@ -1,0 +1,1063 @@
+// Persistent batched solver kernel and the C ABI (include/smili_b200.h).
+//
+// One cooperative launch solves a whole batch: the CTAs are split into groups
+// of G; a group takes the next unsolved problem from a queue and runs
+// function/gradient evaluation (fg.cuh) and L-BFGS-B (lbfgsb.cuh) until the
+// problem stops, then takes the next one.  Stages inside a group are
+// separated by group barriers (common.cuh).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/smili_b200.h"
+#include "common.cuh"
+#include "fft.cuh"
+#include "fg.cuh"
+#include "layout.h"
+#include "lbfgsb.cuh"
+
+#define SMILI_VERSION 1
+#define SMILI_SMEM_CPX 2048   // complex elements per FFT buffer
+#define SMILI_DYN_MIN (40 * 1024)
+
+enum { MODE_SOLVE = 0, MODE_FG = 1, MODE_T2 = 2, MODE_T1 = 3 };
+
+struct BatchArgs {
+  char* arena;
+  const ProbDesc* descs;
+  int nprob, G, mode;
+  int* queue;
+  unsigned* bars;      // [ngroups][2]
+  double* red_part;    // [ngroups][G][SMILI_REDK]
+  double* red_out;     // [ngroups][SMILI_REDK]
+  int* grp_prob;       // [ngroups]
+  int* abort_flag;
+  ProbResult* results; // [nprob]
+};
+
+// ---------------------------------------------------------------------------
+// one function/gradient evaluation by the group (stages F1..F8)
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsigned char* ops,
+                         double* scratch, double& f, double& gd, double& sbg, double* terms,
+                         int mode) {
+  const ProbDesc& P = *fc.P;
+  double mom[10];
+  for (int k = 0; k < 10; ++k) mom[k] = 0.0;
+  fg_t2_rows(fc, g, mom);
+  RegMoments rm;
+  memset(&rm, 0, sizeof(rm));
+  if (P.has_tfd || P.has_cen || P.has_sm) {
+    for (int k = threadIdx.x; k < 10; k += blockDim.x) ops[k] = RED_SUM;
+    __syncthreads();
+    block_reduce_arr(mom, ops, 10, red, scratch);
+    if (!group_reduce(g, red, ops, 10)) return false;
+    double mm[10];
+    for (int k = 0; k < 10; ++k) mm[k] = red[k];
+    reg_moments(P, mm, rm);
+    __syncthreads();
+  } else if (!group_sync(g)) {
+    return false;
+  }
+  fg_t2_cols(fc, g);
+  if (!group_sync(g)) return false;
+  fg_interp(fc, g);
+  if (!group_sync(g)) return false;
+  if (mode == MODE_T2) return true;
+  double chi[4] = {0, 0, 0, 0};
+  if (mode != MODE_T1) {
+    fg_chisq(fc, g, chi);
+    if (!group_sync(g)) return false;
+  }
+  fg_spread(fc, g);
+  if (!group_sync(g)) return false;
+  fg_t1_rows(fc, g);
+  if (!group_sync(g)) return false;
+  fg_t1_cols(fc, g);
+  if (!group_sync(g)) return false;
+  if (mode == MODE_T1) return true;
+  double acc[14];
+  for (int k = 0; k < 14; ++k) acc[k] = 0.0;
+  double reg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  fg_reg_grad(P, fc.base, g, rm, lc.lo, lc.hi, reg, acc[12], acc[13]);
+  for (int k = 0; k < 4; ++k) acc[k] = chi[k];
+  for (int k = 0; k < 8; ++k) acc[4 + k] = reg[k];
+  for (int k = threadIdx.x; k < 14; k += blockDim.x) ops[k] = (k == 13) ? RED_MAX : RED_SUM;
+  __syncthreads();
+  block_reduce_arr(acc, ops, 14, red, scratch);
+  if (!group_reduce(g, red, ops, 14)) return false;
+  double r[14];
+  for (int k = 0; k < 14; ++k) r[k] = red[k];
+  __syncthreads();
+  // global-sum regularizers (image.f90:108-135)
+  if (P.has_tfd) r[4 + 5] = P.tfd_l * rm.tfd_resid * rm.tfd_resid;
+  if (P.has_cen) r[4 + 6] = P.cen_l * rm.cen_cost;
+  if (P.has_sm) {
+    double e = 0;
+    for (int q = 0; q < 2; ++q) e += (rm.Sg[q] - rm.Sp[q]) * (rm.Sg[q] - rm.Sp[q]);
+    e += 2. * (rm.Sg[2] - rm.Sp[2]) * (rm.Sg[2] - rm.Sp[2]);
+    r[4 + 7] = P.sm_l * e;
+  }
+  const double chisq = r[0] + r[1] + r[2] + r[3];
+  double regs = 0;
+  for (int k = 0; k < 8; ++k) regs += r[4 + k];
+  f = chisq + regs;
+  gd = r[12];
+  sbg = r[13];
+  if (threadIdx.x == 0) {
+    terms[0] = chisq;
+    terms[1] = P.nfcv ? r[0] / P.wfcv / (2.0 * P.nfcv) : 0.0;
+    terms[2] = P.namp ? r[1] / P.wamp / P.namp : 0.0;
+    terms[3] = P.ncp ? r[2] / P.wcp / P.ncp : 0.0;
+    terms[4] = P.nca ? r[3] / P.wca / P.nca : 0.0;
+    terms[5] = regs;
+    for (int k = 0; k < 8; ++k) terms[6 + k] = r[4 + k];
+    terms[14] = f;
+  }
+  __syncthreads();
+  return true;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) char dyn[];
+  __shared__ LbState S;
+  __shared__ double red[SMILI_REDK];
+  __shared__ unsigned char ops[SMILI_REDK];
+  __shared__ double scratch[SMILI_WARPS * SMILI_REDK];
+  __shared__ int prob_s;
+  const int grp = blockIdx.x / a.G, rank = blockIdx.x % a.G;
+  GroupCtx g;
+  g.rank = rank;
+  g.G = a.G;
+  g.bar = a.bars + 2 * grp;
+  g.red_part = a.red_part + (size_t)grp * a.G * SMILI_REDK;
+  g.red_out = a.red_out + (size_t)grp * SMILI_REDK;
+  g.abort_flag = a.abort_flag;
+  g.spin_limit = SMILI_SPIN_LIMIT;
+  while (true) {
+    if (rank == 0 && threadIdx.x == 0) {
+      const int p = atomicAdd(a.queue, 1);
+      a.grp_prob[grp] = p;
+      __threadfence();
+    }
+    if (!group_sync(g)) return;
+    if (threadIdx.x == 0) prob_s = ((volatile int*)a.grp_prob)[grp];
+    __syncthreads();
+    const int p = prob_s;
+    if (p >= a.nprob) return;
+    const ProbDesc& P = a.descs[p];
+    char* base = a.arena;
+    FgCtx<R> fc;
+    fc.P = &P;
+    fc.base = base;
+    fc.sbuf = reinterpret_cast<cpx<R>*>(dyn);
+    fc.swork = fc.sbuf + SMILI_SMEM_CPX;
+    fc.smem_cpx = SMILI_SMEM_CPX;
+    LbCtx lc;
+    lc.P = &P;
+    lc.base = base;
+    lc.g = &g;
+    lc.S = &S;
+    lc.n = P.npix;
+    lc.m = P.m;
+    const int chunk = ((P.npix + a.G - 1) / a.G + 31) / 32 * 32;
+    lc.lo = min(P.npix, rank * chunk);
+    lc.hi = min(P.npix, lc.lo + chunk);
+    lc.x = at<double>(base, P.o_x);
+    lc.gv = at<double>(base, P.o_g);
+    lc.z = at<double>(base, P.o_z);
+    lc.r = at<double>(base, P.o_r);
+    lc.d = at<double>(base, P.o_d);
+    lc.t = at<double>(base, P.o_t);
+    lc.xp = at<double>(base, P.o_xp);
+    lc.ws = at<double>(base, P.o_ws);
+    lc.wy = at<double>(base, P.o_wy);
+    lc.iwh = at<signed char>(base, P.o_iwh);
+    lc.freef = at<unsigned char>(base, P.o_free);
+    lc.bkey = at<unsigned long long>(base, P.o_bkey);
+    lc.lred = at<double>(base, P.o_lred);
+    lc.trace = at<double>(base, P.o_trace);
+    lc.red = red;
+    lc.ops = ops;
+    lc.scratch = scratch;
+    lc.dyn = dyn;
+    const double* x0 = at<double>(base, P.o_x0);
+    if (a.mode == MODE_SOLVE) {
+      lb_init(lc, x0);
+      if (rank == 0)
+        for (int i = threadIdx.x; i < P.niter + 2; i += blockDim.x) lc.trace[i] = __longlong_as_double(0x7ff8000000000000LL);
+    } else {
+      // evaluation modes: x as given, no projection
+      for (int i = lc.lo + threadIdx.x; i < lc.hi; i += blockDim.x) {
+        lc.x[i] = x0[i];
+        if (P.o_d) lc.d[i] = 0.0;
+      }
+      if (threadIdx.x == 0) {
+        S.task = LB_TASK_FG_ONLY;
+        S.done = 0;
+        S.error = 0;
+        S.iter = 0;
+        S.nfg_total = 0;
+      }
+      __syncthreads();
+    }
+    bool ok = group_sync(g);
+    double terms_l[SMILI_NTERMS];
+    while (ok) {
+      double f = 0, gd = 0, sbg = 0;
+      if (!group_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms, a.mode)) {
+        ok = false;
+        break;
+      }
+      if (a.mode != MODE_SOLVE) {
+        if (threadIdx.x == 0) S.nfg_total = 1;
+        break;
+      }
+      const int rr = lb_after_fg(lc, f, gd, sbg);
+      if (S.error) ok = false;
+      if (rr != LB_RET_FG) break;
+      if (!group_sync(g)) ok = false;
+    }
+    if (ok && a.mode == MODE_SOLVE) {
+      // final summary evaluation at the returned image (fftim2d.f90:356-376)
+      if (!group_sync(g)) ok = false;
+      double f = 0, gd = 0, sbg = 0;
+      if (ok && !group_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms, MODE_FG)) ok = false;
+      if (threadIdx.x == 0) S.nfg_total++;
+    }
+    (void)terms_l;
+    __syncthreads();
+    if (rank == 0 && threadIdx.x == 0) {
+      ProbResult& res = a.results[p];
+      for (int k = 0; k < SMILI_NTERMS; ++k) res.terms[k] = S.terms[k];
+      res.task = ok ? S.task : LB_TASK_ERROR;
+      res.iter = S.iter;
+      res.nfg = S.nfg_total;
+      res.error = ok ? S.error : 1;
+    }
+    if (!ok) return;
+    if (!group_sync(g)) return;
+  }
+}
+
+// ===========================================================================
+// host side
+// ===========================================================================
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(SMILI_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+int next235even(int n) {
+  if (n <= 2) return 2;
+  if (n % 2) n += 1;
+  for (int m = n;; m += 2) {
+    int k = m;
+    for (int p : {2, 3, 5})
+      while (k % p == 0) k /= p;
+    if (k == 1) return m;
+  }
+}
+
+void es_params(double eps, int& w, double& beta) {
+  w = (int)std::ceil(std::log10(10.0 / eps));
+  w = std::max(2, std::min(SMILI_MAXW, w));
+  double c = 2.30;
+  if (w == 2) c = 2.20;
+  else if (w == 3) c = 2.26;
+  else if (w == 4) c = 2.38;
+  beta = c * w;
+}
+
+// Gauss-Legendre nodes on (0, 1] of a q-point rule on [-1, 1]
+void gl_positive(int q, std::vector<double>& x, std::vector<double>& wt) {
+  x.clear();
+  wt.clear();
+  for (int i = 0; i < q; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (q + 0.5));
+    double dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= q; ++k) {
+        const double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = q * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    double p0 = 1.0, p1 = z;
+    for (int k = 2; k <= q; ++k) {
+      const double p2 = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    dp = q * (z * p1 - p0) / (z * z - 1.0);
+    if (z > 0) {
+      x.push_back(z);
+      wt.push_back(2.0 / ((1 - z * z) * dp * dp));
+    }
+  }
+}
+
+// 1 / psi_hat(k) for the N modes k = -N/2..(N-1)/2 on a fine grid of nf cells
+std::vector<double> deconv_factors(int N, int nf, int w, double beta) {
+  std::vector<double> gx, gw;
+  gl_positive(80, gx, gw);
+  std::vector<double> out(N);
+  for (int i = 0; i < N; ++i) {
+    const int k = i - N / 2;
+    double acc = 0;
+    for (size_t q = 0; q < gx.size(); ++q) {
+      const double z = gx[q], s = 1.0 - z * z;
+      const double phi = s > 0 ? std::exp(beta * (std::sqrt(s) - 1.0)) : 0.0;
+      acc += gw[q] * phi * std::cos(M_PI * k * w * z / nf);
+    }
+    out[i] = 1.0 / (w * acc);
+  }
+  return out;
+}
+
+struct Arena {
+  size_t bytes = 0;
+  int64_t take(size_t nbytes) {
+    const int64_t off = (int64_t)bytes;
+    bytes += (nbytes + 255) / 256 * 256;
+    return off;
+  }
+};
+
+bool finite_all(const double* p, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+// Host image of one problem: descriptor + the byte blobs to upload
+struct HostProb {
+  ProbDesc d;
+  std::vector<std::pair<int64_t, std::vector<char>>> blobs;
+  template <typename T>
+  void put(int64_t off, const std::vector<T>& v) {
+    std::vector<char> b(v.size() * sizeof(T));
+    if (!v.empty()) std::memcpy(b.data(), v.data(), b.size());
+    blobs.emplace_back(off, std::move(b));
+  }
+};
+
+enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3 };
+
+template <typename R>
+int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, int m, double factr,
+                 double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override,
+                 const double* c_re, const double* c_im) {
+  ProbDesc& d = hp.d;
+  std::memset(&d, 0, sizeof(d));
+  const int N = a.npix, nx = a.nx, ny = a.ny, nuv = a.nuv;
+  if (N < 1 || nx < 1 || ny < 1 || nuv < 1 || (long)N > (long)nx * ny)
+    return fail(SMILI_ERR_ARG, "invalid image or uv sizes");
+  if (m < 1 || m > SMILI_MAXM_DEV) return fail(SMILI_ERR_UNSUPPORTED, "L-BFGS-B memory m must be 1..6");
+  if (!a.iin || !a.xidx || !a.yidx || !a.u || !a.v) return fail(SMILI_ERR_ARG, "null array");
+  std::vector<int> inv((size_t)nx * ny, -1);
+  std::vector<int> xi(N), yi(N);
+  for (int i = 0; i < N; ++i) {
+    const int ix = a.xidx[i] - 1, iy = a.yidx[i] - 1;
+    if (ix < 0 || ix >= nx || iy < 0 || iy >= ny) return fail(SMILI_ERR_ARG, "xidx/yidx out of range");
+    if (inv[(size_t)iy * nx + ix] >= 0) return fail(SMILI_ERR_ARG, "duplicate pixel in xidx/yidx");
+    inv[(size_t)iy * nx + ix] = i;
+    xi[i] = ix;
+    yi[i] = iy;
+  }
+  const double* x0 = x_override ? x_override : a.iin;
+  if (!finite_all(x0, N) || !finite_all(a.u, nuv) || !finite_all(a.v, nuv))
+    return fail(SMILI_ERR_DATA, "non-finite image or uv coordinates");
+  // NUFFT parameters
+  int w;
+  double beta;
+  es_params(eps, w, beta);
+  d.w = w;
+  d.beta = beta;
+  d.nf1 = next235even(std::max(2 * nx, 2 * w));
+  d.nf2 = next235even(std::max(2 * ny, 2 * w));
+  if (d.nf1 > SMILI_SMEM_CPX || d.nf2 > SMILI_SMEM_CPX)
+    return fail(SMILI_ERR_UNSUPPORTED, "fine grid larger than 2048 cells per axis");
+  d.npix = N;
+  d.nx = nx;
+  d.ny = ny;
+  d.nuv = nuv;
+  d.m = m;
+  d.niter = niter;
+  d.nonneg = nonneg ? 1 : 0;
+  d.factr = factr;
+  d.pgtol = pgtol;
+  d.prec64 = sizeof(R) == 8;
+  d.nxref = a.nxref;
+  d.nyref = a.nyref;
+  d.windowed = N != nx * ny;
+  // data terms
+  const bool use_data = kind == PK_SOLVE || kind == PK_FG;
+  const int nfcv = (use_data && a.isfcv) ? a.nfcv : 0;
+  const int namp = (use_data && a.isamp) ? a.namp : 0;
+  const int ncp = (use_data && a.iscp) ? a.ncp : 0;
+  const int nca = (use_data && a.isca) ? a.nca : 0;
+  if (use_data && nfcv + namp + ncp + nca == 0) return fail(SMILI_ERR_ARG, "no data terms");
+  d.nfcv = nfcv;
+  d.namp = namp;
+  d.ncp = ncp;
+  d.nca = nca;
+  d.ndata = nfcv + namp + ncp + nca;
+  const int nslot = (kind == PK_T1) ? nuv : nfcv + namp + 3 * ncp + 4 * nca;
+  d.nslot = nslot;
+  // normalised data weights (fftim2d.f90:178-213)
+  double wtotal = 0;
+  if (nfcv) wtotal += 2.0 * nfcv * a.wfcv;
+  if (namp) wtotal += (double)namp * a.wamp;
+  if (ncp) wtotal += (double)ncp * a.wcp;
+  if (nca) wtotal += (double)nca * a.wca;
+  d.wfcv = nfcv ? a.wfcv / wtotal : 0;
+  d.wamp = namp ? a.wamp / wtotal : 0;
+  d.wcp = ncp ? a.wcp / wtotal : 0;
+  d.wca = nca ? a.wca / wtotal : 0;
+  // regularizers (active when lambda > 0, image.f90:112-175)
+  const bool use_reg = kind == PK_SOLVE || kind == PK_FG;
+  auto need_w = [&](double l, const double* wv, int nw, const char* nm) -> int {
+    if (!(use_reg && l > 0)) return 0;
+    if (!wv || nw != N) return fail(SMILI_ERR_ARG, std::string(nm) + " weights must have npix entries");
+    if (!finite_all(wv, N)) return fail(SMILI_ERR_DATA, std::string(nm) + " weights not finite");
+    return 1;
+  };
+  int rc;
+  if ((rc = need_w(a.l1_l, a.l1_wgt, a.l1_nwgt, "l1")) < 0) return rc;
+  d.has_l1 = rc;
+  if ((rc = need_w(a.tv_l, a.tv_wgt, a.tv_nwgt, "tv")) < 0) return rc;
+  d.has_tv = rc;
+  if ((rc = need_w(a.tsv_l, a.tsv_wgt, a.tsv_nwgt, "tsv")) < 0) return rc;
+  d.has_tsv = rc;
+  if ((rc = need_w(a.kl_l, a.kl_wgt, a.kl_nwgt, "kl")) < 0) return rc;
+  d.has_kl = rc;
+  if ((rc = need_w(a.gs_l, a.gs_wgt, a.gs_nwgt, "gs")) < 0) return rc;
+  d.has_gs = rc;
+  d.has_tfd = use_reg && a.tfd_l > 0;
+  d.has_cen = use_reg && a.cen_l > 0;
+  d.has_sm = use_reg && a.sm_l > 0;
+  d.l1_l = a.l1_l;
+  d.tv_l = a.tv_l;
+  d.tsv_l = a.tsv_l;
+  d.kl_l = a.kl_l;
+  d.gs_l = a.gs_l;
+  d.tfd_l = a.tfd_l;
+  d.tfd_tgtfd = a.tfd_tgtfd;
+  d.cen_l = a.cen_l;
+  d.cen_alpha = a.cen_alpha;
+  d.sm_l = a.sm_l;
+  d.sm_maj = a.sm_maj;
+  d.sm_min = a.sm_min;
+  d.sm_phi = a.sm_phi;
+
+  // fine-grid coordinates in the kernel precision, band of touched cells
+  std::vector<R> xu(nuv), xv(nuv);
+  const R half = (R)0.5 * (R)w;
+  long mn1 = 1L << 40, mx1 = -(1L << 40), mn2 = 1L << 40, mx2 = -(1L << 40);
+  for (int j = 0; j < nuv; ++j) {
+    xu[j] = (R)(a.u[j] * d.nf1 / (2.0 * M_PI));
+    xv[j] = (R)(a.v[j] * d.nf2 / (2.0 * M_PI));
+    const long l1 = (long)std::ceil(xu[j] - half), l2 = (long)std::ceil(xv[j] - half);
+    mn1 = std::min(mn1, l1);
+    mx1 = std::max(mx1, l1 + w - 1);
+    mn2 = std::min(mn2, l2);
+    mx2 = std::max(mx2, l2 + w - 1);
+  }
+  if (mx1 - mn1 + 1 >= d.nf1) {
+    d.b1s = 0;
+    d.b1n = d.nf1;
+  } else {
+    d.b1s = (int)mn1;
+    d.b1n = (int)(mx1 - mn1 + 1);
+  }
+  if (mx2 - mn2 + 1 >= d.nf2) {
+    d.b2s = 0;
+    d.b2n = d.nf2;
+  } else {
+    d.b2s = (int)mn2;
+    d.b2n = (int)(mx2 - mn2 + 1);
+  }
+  // sort the uv points by 8x8 tiles of the band for locality; remap indices
+  std::vector<int> perm(nuv);
+  std::iota(perm.begin(), perm.end(), 0);
+  {
+    std::vector<long> key(nuv);
+    for (int j = 0; j < nuv; ++j) {
+      const long c1 = (long)std::ceil(xu[j] - half) - d.b1s, c2 = (long)std::ceil(xv[j] - half) - d.b2s;
+      key[j] = ((c2 >> 3) << 32) + (c1 >> 3);
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](int p, int q) { return key[p] < key[q]; });
+  }
+  std::vector<int> newpos(nuv);
+  for (int j = 0; j < nuv; ++j) newpos[perm[j]] = j;
+  std::vector<R> su(nuv), sv(nuv);
+  for (int j = 0; j < nuv; ++j) {
+    su[j] = xu[perm[j]];
+    sv[j] = xv[perm[j]];
+  }
+  // data: values, variances, slots
+  std::vector<R> dre(std::max(d.ndata, 1)), dim(std::max(d.ndata, 1)), dvar(std::max(d.ndata, 1));
+  std::vector<int> didx(std::max(nslot, 1));
+  std::vector<signed char> dsgn(std::max(nslot, 1));
+  auto slot = [&](int s, int uvidx) -> int {
+    if (uvidx == 0 || std::abs(uvidx) > nuv) return fail(SMILI_ERR_ARG, "uv index out of range");
+    didx[s] = newpos[std::abs(uvidx) - 1];
+    dsgn[s] = uvidx > 0 ? 1 : -1;
+    return 0;
+  };
+  auto check_var = [&](double v) { return std::isfinite(v) && v > 0.0; };
+  int e = 0, s = 0;
+  if (nfcv) {
+    if (!a.uvidxfcv || !a.vfcvr || !a.vfcvi || !a.varfcv) return fail(SMILI_ERR_ARG, "null fcv array");
+    const double dix = a.nxref - nx / 2.0 - 1, diy = a.nyref - ny / 2.0 - 1;
+    for (int i = 0; i < nfcv; ++i, ++e, ++s) {
+      if ((rc = slot(s, a.uvidxfcv[i])) < 0) return rc;
+      const int k = std::abs(a.uvidxfcv[i]) - 1, sg = a.uvidxfcv[i] > 0 ? 1 : -1;
+      if (!std::isfinite(a.vfcvr[i]) || !std::isfinite(a.vfcvi[i]) || !check_var(a.varfcv[i]))
+        return fail(SMILI_ERR_DATA, "invalid complex visibility or variance");
+      // phashift_r2c (fftlib.f90:223-244)
+      const std::complex<double> z = std::complex<double>(a.vfcvr[i], a.vfcvi[i]) *
+                                     std::exp(std::complex<double>(0.0, a.u[k] * sg * dix + a.v[k] * sg * diy));
+      dre[e] = (R)z.real();
+      dim[e] = (R)z.imag();
+      dvar[e] = (R)a.varfcv[i];
+    }
+  }
+  if (namp) {
+    if (!a.uvidxamp || !a.vamp || !a.varamp) return fail(SMILI_ERR_ARG, "null amp array");
+    for (int i = 0; i < namp; ++i, ++e, ++s) {
+      if ((rc = slot(s, a.uvidxamp[i])) < 0) return rc;
+      if (!std::isfinite(a.vamp[i]) || !check_var(a.varamp[i]))
+        return fail(SMILI_ERR_DATA, "invalid amplitude or variance");
+      dre[e] = (R)a.vamp[i];
+      dim[e] = 0;
+      dvar[e] = (R)a.varamp[i];
+    }
+  }
+  if (ncp) {
+    if (!a.uvidxcp || !a.cp || !a.varcp) return fail(SMILI_ERR_ARG, "null cp array");
+    for (int i = 0; i < ncp; ++i, ++e) {
+      for (int q = 0; q < 3; ++q, ++s)
+        if ((rc = slot(s, a.uvidxcp[3 * i + q])) < 0) return rc;
+      if (!std::isfinite(a.cp[i]) || !check_var(a.varcp[i]))
+        return fail(SMILI_ERR_DATA, "invalid closure phase or variance");
+      dre[e] = (R)a.cp[i];
+      dim[e] = 0;
+      dvar[e] = (R)a.varcp[i];
+    }
+  }
+  if (nca) {
+    if (!a.uvidxca || !a.ca || !a.varca) return fail(SMILI_ERR_ARG, "null ca array");
+    for (int i = 0; i < nca; ++i, ++e) {
+      for (int q = 0; q < 4; ++q, ++s)
+        if ((rc = slot(s, a.uvidxca[4 * i + q])) < 0) return rc;
+      if (!std::isfinite(a.ca[i]) || !check_var(a.varca[i]))
+        return fail(SMILI_ERR_DATA, "invalid closure amplitude or variance");
+      dre[e] = (R)a.ca[i];
+      dim[e] = 0;
+      dvar[e] = (R)a.varca[i];
+    }
+  }
+  // uv point -> contribution slots (CSR); for the bare type-1 mode the slots
+  // are the uv points themselves with contrib = (Re c, -Im c)
+  std::vector<int> csr_off(nuv + 1, 0), csr_ent(std::max(nslot, 1));
+  std::vector<cpx<R>> contrib0;
+  if (kind == PK_T1) {
+    for (int j = 0; j <= nuv; ++j) csr_off[j] = j;
+    contrib0.resize(nuv);
+    for (int j = 0; j < nuv; ++j) {
+      const int o = perm[j];
+      csr_ent[j] = j;
+      contrib0[j].x = (R)c_re[o];
+      contrib0[j].y = (R)(-c_im[o]);
+    }
+  } else {
+    for (int q = 0; q < nslot; ++q) csr_off[didx[q] + 1]++;
+    for (int j = 0; j < nuv; ++j) csr_off[j + 1] += csr_off[j];
+    std::vector<int> fillp(csr_off.begin(), csr_off.end() - 1);
+    for (int q = 0; q < nslot; ++q) csr_ent[fillp[didx[q]]++] = q;
+  }
+  // deconvolution factors and twiddles
+  const std::vector<double> dc1 = deconv_factors(nx, d.nf1, w, beta), dc2 = deconv_factors(ny, d.nf2, w, beta);
+  auto twiddles = [](int n) {
+    std::vector<cpx<R>> t(n);
+    for (int k = 0; k < n; ++k) {
+      const long double ang = 2.0L * 3.14159265358979323846264338327950288L * k / n;
+      t[k].x = (R)std::cos(ang);
+      t[k].y = (R)std::sin(ang);
+    }
+    return t;
+  };
+  // ---- arena layout ----
+  const size_t C = sizeof(cpx<R>);
+  d.o_x0 = ar.take(sizeof(double) * N);
+  d.o_xidx = ar.take(sizeof(int) * N);
+  d.o_yidx = ar.take(sizeof(int) * N);
+  d.o_inv = ar.take(sizeof(int) * (size_t)nx * ny);
+  if (d.has_l1) d.o_l1w = ar.take(sizeof(double) * N);
+  if (d.has_tv) d.o_tvw = ar.take(sizeof(double) * N);
+  if (d.has_tsv) d.o_tsvw = ar.take(sizeof(double) * N);
+  if (d.has_kl) d.o_klw = ar.take(sizeof(double) * N);
+  if (d.has_gs) d.o_gsw = ar.take(sizeof(double) * N);
+  d.o_dc1 = ar.take(sizeof(double) * nx);
+  d.o_dc2 = ar.take(sizeof(double) * ny);
+  d.o_tw1 = ar.take(C * d.nf1);
+  d.o_tw2 = ar.take(C * d.nf2);
+  d.o_u = ar.take(sizeof(R) * nuv);
+  d.o_v = ar.take(sizeof(R) * nuv);
+  d.o_dre = ar.take(sizeof(R) * dre.size());
+  d.o_dim = ar.take(sizeof(R) * dim.size());
+  d.o_dvar = ar.take(sizeof(R) * dvar.size());
+  d.o_didx = ar.take(sizeof(int) * didx.size());
+  d.o_dsgn = ar.take(dsgn.size());
+  d.o_csr_off = ar.take(sizeof(int) * (nuv + 1));
+  d.o_csr_ent = ar.take(sizeof(int) * csr_ent.size());
+  d.o_tmpA = ar.take(C * (size_t)ny * d.b1n);
+  d.o_bandA = ar.take(C * (size_t)d.b2n * d.b1n);
+  d.o_V = ar.take(C * nuv);
+  d.o_contrib = ar.take(C * std::max(nslot, 1));
+  d.o_bandC = ar.take(C * (size_t)d.b2n * d.b1n);
+  d.o_tmpC = ar.take(C * (size_t)d.b2n * nx);
+  d.o_gchi = ar.take(sizeof(double) * (size_t)nx * ny);
+  d.o_x = ar.take(sizeof(double) * N);
+  d.o_g = ar.take(sizeof(double) * N);
+  if (kind == PK_SOLVE || kind == PK_FG) {
+    d.o_z = ar.take(sizeof(double) * N);
+    d.o_r = ar.take(sizeof(double) * N);
+    d.o_d = ar.take(sizeof(double) * N);
+    d.o_t = ar.take(sizeof(double) * N);
+    d.o_xp = ar.take(sizeof(double) * N);
+    d.o_iwh = ar.take(N);
+    d.o_free = ar.take(N);
+    d.o_bkey = ar.take(sizeof(unsigned long long) * N);
+    d.o_lred = ar.take(sizeof(double) * 64);
+    d.o_trace = ar.take(sizeof(double) * (niter + 2));
+  }
+  if (kind == PK_SOLVE) {
+    d.o_ws = ar.take(sizeof(double) * (size_t)N * m);
+    d.o_wy = ar.take(sizeof(double) * (size_t)N * m);
+  }
+  // ---- blobs ----
+  hp.put(d.o_x0, std::vector<double>(x0, x0 + N));
+  hp.put(d.o_xidx, xi);
+  hp.put(d.o_yidx, yi);
+  hp.put(d.o_inv, inv);
+  if (d.has_l1) hp.put(d.o_l1w, std::vector<double>(a.l1_wgt, a.l1_wgt + N));
+  if (d.has_tv) hp.put(d.o_tvw, std::vector<double>(a.tv_wgt, a.tv_wgt + N));
+  if (d.has_tsv) hp.put(d.o_tsvw, std::vector<double>(a.tsv_wgt, a.tsv_wgt + N));
+  if (d.has_kl) hp.put(d.o_klw, std::vector<double>(a.kl_wgt, a.kl_wgt + N));
+  if (d.has_gs) hp.put(d.o_gsw, std::vector<double>(a.gs_wgt, a.gs_wgt + N));
+  hp.put(d.o_dc1, dc1);
+  hp.put(d.o_dc2, dc2);
+  hp.put(d.o_tw1, twiddles(d.nf1));
+  hp.put(d.o_tw2, twiddles(d.nf2));
+  hp.put(d.o_u, su);
+  hp.put(d.o_v, sv);
+  hp.put(d.o_dre, dre);
+  hp.put(d.o_dim, dim);
+  hp.put(d.o_dvar, dvar);
+  hp.put(d.o_didx, didx);
+  hp.put(d.o_dsgn, dsgn);
+  hp.put(d.o_csr_off, csr_off);
+  hp.put(d.o_csr_ent, csr_ent);
+  if (kind == PK_T1) hp.put(d.o_contrib, contrib0);
+  // the original -> sorted uv permutation is needed to return visibilities
+  hp.blobs.emplace_back(-1, std::vector<char>((const char*)perm.data(), (const char*)perm.data() + sizeof(int) * nuv));
+  return SMILI_OK;
+}
+
+}  // namespace
+
+struct smili_batch {
+  int nprob = 0, prec64 = 1, G = 1, ngroups = 1, device = 0;
+  int kind = PK_SOLVE;
+  std::vector<ProbDesc> descs;
+  std::vector<std::vector<int>> perms;
+  char* d_arena = nullptr;
+  size_t arena_bytes = 0;
+  ProbDesc* d_descs = nullptr;
+  char* d_aux = nullptr;  // queue, bars, reductions, results
+  ProbResult* d_results = nullptr;
+  int* d_queue = nullptr;
+  unsigned* d_bars = nullptr;
+  double* d_red_part = nullptr;
+  double* d_red_out = nullptr;
+  int* d_grp_prob = nullptr;
+  int* d_abort = nullptr;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  size_t dyn_bytes = 0;
+};
+
+namespace {
+
+template <typename R>
+int launch_batch(smili_batch* b, int mode, float* ms) {
+  const void* fn = (const void*)smili_batch_kernel<R>;
+  const size_t aux_reset = 0;
+  (void)aux_reset;
+  CUDA_TRY(cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream));
+  CUDA_TRY(cudaMemsetAsync(b->d_bars, 0, sizeof(unsigned) * 2 * b->ngroups, b->stream));
+  CUDA_TRY(cudaMemsetAsync(b->d_abort, 0, sizeof(int), b->stream));
+  BatchArgs a;
+  a.arena = b->d_arena;
+  a.descs = b->d_descs;
+  a.nprob = b->nprob;
+  a.G = b->G;
+  a.mode = mode;
+  a.queue = b->d_queue;
+  a.bars = b->d_bars;
+  a.red_part = b->d_red_part;
+  a.red_out = b->d_red_out;
+  a.grp_prob = b->d_grp_prob;
+  a.abort_flag = b->d_abort;
+  a.results = b->d_results;
+  void* args[] = {&a};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ms) {
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, b->stream));
+  }
+  CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(b->G * b->ngroups), dim3(SMILI_THREADS), args,
+                                       b->dyn_bytes, b->stream));
+  if (ms) {
+    CUDA_TRY(cudaEventRecord(e1, b->stream));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    CUDA_TRY(cudaEventElapsedTime(ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  int abort_flag = 0;
+  CUDA_TRY(cudaMemcpy(&abort_flag, b->d_abort, sizeof(int), cudaMemcpyDeviceToHost));
+  if (abort_flag) return fail(SMILI_ERR_TIMEOUT, "a device-side group barrier timed out; solve aborted");
+  return SMILI_OK;
+}
+
+template <typename R>
+int create_batch(int nprob, const smili_imaging_args* const* probs, const int* niter, int nonneg,
+                 int m, double factr, double pgtol, const smili_options* opt, int kind,
+                 const double* const* x_over, const double* c_re, const double* c_im,
+                 smili_batch** out) {
+  const double eps = (opt && opt->nufft_eps > 0) ? opt->nufft_eps : 1e-6;
+  const int device = opt ? opt->device : 0;
+  if (!(eps < 1.0)) return fail(SMILI_ERR_ARG, "nufft_eps must be in (0, 1)");
+  smili_batch* b = new smili_batch();
+  b->nprob = nprob;
+  b->prec64 = sizeof(R) == 8;
+  b->device = device;
+  b->kind = kind;
+  Arena ar;
+  std::vector<HostProb> hps(nprob);
+  int maxn = 1;
+  for (int p = 0; p < nprob; ++p) {
+    const int rc = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ar,
+                                   hps[p], x_over ? x_over[p] : nullptr, c_re, c_im);
+    if (rc != SMILI_OK) {
+      delete b;
+      return rc;
+    }
+    b->descs.push_back(hps[p].d);
+    maxn = std::max(maxn, hps[p].d.npix);
+  }
+  b->arena_bytes = ar.bytes;
+  // inputs are valid: now the device
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) {
+    delete b;
+    return fail(SMILI_ERR_NODEV, "no CUDA device");
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete b;
+    return fail(SMILI_ERR_NODEV, "cannot select the CUDA device");
+  }
+  // launch geometry: co-resident CTAs split into groups
+  b->dyn_bytes = std::max((size_t)SMILI_DYN_MIN, 2 * (size_t)SMILI_SMEM_CPX * sizeof(cpx<R>));
+  const void* fn = (const void*)smili_batch_kernel<R>;
+  auto cleanup = [&](int rc) {
+    smili_batch_destroy(b);
+    return rc;
+  };
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_bytes) != cudaSuccess)
+    return cleanup(fail(SMILI_ERR_CUDA, "cannot set dynamic shared memory size"));
+  int occ = 0, nsm = 0, coop = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, SMILI_THREADS, b->dyn_bytes));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  if (!coop || occ < 1) return cleanup(fail(SMILI_ERR_CUDA, "cooperative launch unavailable"));
+  const int maxres = occ * nsm;
+  int G = opt && opt->ctas_per_problem > 0 ? opt->ctas_per_problem : 0;
+  if (G <= 0) {
+    G = std::max(1, std::min(maxres, (maxn + 1023) / 1024));
+    if (nprob > 1) G = std::max(1, std::min(G, maxres / nprob));
+  }
+  G = std::min(G, maxres);
+  b->G = G;
+  b->ngroups = std::max(1, std::min(nprob, maxres / G));
+  // device buffers
+  if (cudaMalloc(&b->d_arena, std::max<size_t>(b->arena_bytes, 256)) != cudaSuccess)
+    return cleanup(fail(SMILI_ERR_CUDA, "cudaMalloc of the problem arena failed"));
+  size_t aux = 0;
+  auto take = [&](size_t n) {
+    const size_t o = aux;
+    aux += (n + 255) / 256 * 256;
+    return o;
+  };
+  const size_t o_desc = take(sizeof(ProbDesc) * nprob), o_res = take(sizeof(ProbResult) * nprob),
+               o_q = take(sizeof(int)), o_bar = take(sizeof(unsigned) * 2 * b->ngroups),
+               o_rp = take(sizeof(double) * (size_t)b->ngroups * G * SMILI_REDK),
+               o_ro = take(sizeof(double) * (size_t)b->ngroups * SMILI_REDK),
+               o_gp = take(sizeof(int) * b->ngroups), o_ab = take(sizeof(int));
+  if (cudaMalloc(&b->d_aux, aux) != cudaSuccess) return cleanup(fail(SMILI_ERR_CUDA, "cudaMalloc aux failed"));
+  b->d_descs = reinterpret_cast<ProbDesc*>(b->d_aux + o_desc);
+  b->d_results = reinterpret_cast<ProbResult*>(b->d_aux + o_res);
+  b->d_queue = reinterpret_cast<int*>(b->d_aux + o_q);
+  b->d_bars = reinterpret_cast<unsigned*>(b->d_aux + o_bar);
+  b->d_red_part = reinterpret_cast<double*>(b->d_aux + o_rp);
+  b->d_red_out = reinterpret_cast<double*>(b->d_aux + o_ro);
+  b->d_grp_prob = reinterpret_cast<int*>(b->d_aux + o_gp);
+  b->d_abort = reinterpret_cast<int*>(b->d_aux + o_ab);
+  if (opt && opt->stream) {
+    b->stream = (cudaStream_t)opt->stream;
+  } else {
+    CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->own_stream = true;
+  }
+  // upload: zero the arena, then every blob
+  CUDA_TRY(cudaMemsetAsync(b->d_arena, 0, b->arena_bytes, b->stream));
+  for (int p = 0; p < nprob; ++p) {
+    for (auto& bl : hps[p].blobs) {
+      if (bl.first < 0) {
+        b->perms.emplace_back((const int*)bl.second.data(), (const int*)(bl.second.data() + bl.second.size()));
+        continue;
+      }
+      if (!bl.second.empty())
+        CUDA_TRY(cudaMemcpyAsync(b->d_arena + bl.first, bl.second.data(), bl.second.size(),
+                                 cudaMemcpyHostToDevice, b->stream));
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(b->d_descs, b->descs.data(), sizeof(ProbDesc) * nprob, cudaMemcpyHostToDevice,
+                           b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
+  *out = b;
+  return SMILI_OK;
+}
+
+int run(smili_batch* b, int mode, float* ms) {
+  CUDA_TRY(cudaSetDevice(b->device));
+  return b->prec64 ? launch_batch<double>(b, mode, ms) : launch_batch<float>(b, mode, ms);
+}
+
+int create_any(int nprob, const smili_imaging_args* const* probs, const int* niter, int nonneg, int m,
+               double factr, double pgtol, const smili_options* opt, int kind, const double* const* x_over,
+               const double* c_re, const double* c_im, smili_batch** out) {
+  if (nprob < 1 || !probs || !out) return fail(SMILI_ERR_ARG, "invalid batch arguments");
+  const int prec = opt && opt->precision ? opt->precision : 64;
+  if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
+  if (prec == 64)
+    return create_batch<double>(nprob, probs, niter, nonneg, m, factr, pgtol, opt, kind, x_over, c_re, c_im, out);
+  return create_batch<float>(nprob, probs, niter, nonneg, m, factr, pgtol, opt, kind, x_over, c_re, c_im, out);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* smili_last_error(void) { return g_err.c_str(); }
+int smili_version(void) { return SMILI_VERSION; }
+
+int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const int* niter, int nonneg,
+                       int m, double factr, double pgtol, const smili_options* opt, smili_batch** out) {
+  return create_any(nprob, probs, niter, nonneg, m, factr, pgtol, opt, PK_SOLVE, nullptr, nullptr, nullptr,
+                    out);
+}
+
+int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms) {
+  if (!b) return fail(SMILI_ERR_ARG, "null batch");
+  return run(b, fg_only ? MODE_FG : MODE_SOLVE, kernel_ms);
+}
+
+int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double* grad,
+                      smili_solve_info* info) {
+  if (!b || p < 0 || p >= b->nprob) return fail(SMILI_ERR_ARG, "invalid problem index");
+  CUDA_TRY(cudaSetDevice(b->device));
+  const ProbDesc& d = b->descs[p];
+  if (iout) CUDA_TRY(cudaMemcpy(iout, b->d_arena + d.o_x, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
+  if (grad) CUDA_TRY(cudaMemcpy(grad, b->d_arena + d.o_g, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
+  ProbResult r;
+  CUDA_TRY(cudaMemcpy(&r, b->d_results + p, sizeof(r), cudaMemcpyDeviceToHost));
+  if (terms) std::memcpy(terms, r.terms, sizeof(double) * SMILI_NTERMS);
+  if (info) {
+    info->task = r.task;
+    info->niter = r.iter;
+    info->nfg = r.nfg;
+    info->error = r.error;
+  }
+  return SMILI_OK;
+}
+
+int smili_batch_trace(smili_batch* b, int p, double* trace, int len) {
+  if (!b || p < 0 || p >= b->nprob || !trace) return fail(SMILI_ERR_ARG, "invalid trace request");
+  const ProbDesc& d = b->descs[p];
+  if (!d.o_trace) return fail(SMILI_ERR_ARG, "no trace for this batch");
+  const int n = std::min(len, d.niter + 2);
+  CUDA_TRY(cudaSetDevice(b->device));
+  CUDA_TRY(cudaMemcpy(trace, b->d_arena + d.o_trace, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  for (int i = n; i < len; ++i) trace[i] = NAN;
+  return SMILI_OK;
+}
+
+void smili_batch_destroy(smili_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->d_arena) cudaFree(b->d_arena);
+  if (b->d_aux) cudaFree(b->d_aux);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int smili_fftim2d_imaging(const smili_imaging_args* a, int niter, int nonneg, int nprint, int m, double factr,
+                          double pgtol, const smili_options* opt, double* iout, double* terms,
+                          smili_solve_info* info) {
+  (void)nprint;  // progress prints re-evaluate the cost at the same image; no effect on the result
+  if (!a || !iout) return fail(SMILI_ERR_ARG, "null argument");
+  if (niter < 0) return fail(SMILI_ERR_ARG, "niter must be >= 0");
+  smili_batch* b = nullptr;
+  const smili_imaging_args* probs[1] = {a};
+  int rc = create_any(1, probs, &niter, nonneg, m, factr, pgtol, opt, PK_SOLVE, nullptr, nullptr, nullptr, &b);
+  if (rc != SMILI_OK) return rc;
+  rc = run(b, MODE_SOLVE, nullptr);
+  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, iout, terms, nullptr, info);
+  smili_batch_destroy(b);
+  return rc;
+}
+
+int smili_calc_cost(const smili_imaging_args* a, const double* x, const smili_options* opt, double* terms,
+                    double* grad) {
+  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+  smili_batch* b = nullptr;
+  const smili_imaging_args* probs[1] = {a};
+  const double* xo[1] = {x};
+  int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_FG, xo, nullptr, nullptr, &b);
+  if (rc != SMILI_OK) return rc;
+  rc = run(b, MODE_FG, nullptr);
+  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
+  smili_batch_destroy(b);
+  return rc;
+}
+
+static smili_imaging_args bare_args(int nuv, const double* u, const double* v, int nx, int ny,
+                                    std::vector<double>& img, std::vector<int>& xi, std::vector<int>& yi) {
+  smili_imaging_args a;
+  std::memset(&a, 0, sizeof(a));
+  a.npix = nx * ny;
+  a.nx = nx;
+  a.ny = ny;
+  xi.resize(a.npix);
+  yi.resize(a.npix);
+  for (int i = 0; i < a.npix; ++i) {
+    xi[i] = i % nx + 1;
+    yi[i] = i / nx + 1;
+  }
+  if ((int)img.size() < a.npix) img.resize(a.npix, 0.0);
+  a.iin = img.data();
+  a.xidx = xi.data();
+  a.yidx = yi.data();
+  a.nxref = nx / 2 + 1;
+  a.nyref = ny / 2 + 1;
+  a.nuv = nuv;
+  a.u = u;
+  a.v = v;
+  return a;
+}
+
+int smili_nufft_fwd_real(int nuv, const double* u, const double* v, int nx, int ny, const double* img,
+                         const smili_options* opt, double* vreal, double* vimag) {
+  if (!u || !v || !img || !vreal || !vimag || nx < 1 || ny < 1 || nuv < 1)
+    return fail(SMILI_ERR_ARG, "invalid nufft arguments");
+  std::vector<double> im(img, img + (size_t)nx * ny);
+  std::vector<int> xi, yi;
+  smili_imaging_args a = bare_args(nuv, u, v, nx, ny, im, xi, yi);
+  smili_batch* b = nullptr;
+  const smili_imaging_args* probs[1] = {&a};
+  int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_T2, nullptr, nullptr, nullptr, &b);
+  if (rc != SMILI_OK) return rc;
+  // x = image in evaluation mode
+  rc = run(b, MODE_T2, nullptr);
+  if (rc == SMILI_OK) {
+    const ProbDesc& d = b->descs[0];
+    const size_t C = b->prec64 ? 16 : 8;
+    std::vector<char> buf(C * nuv);
+    cudaError_t e = cudaMemcpy(buf.data(), b->d_arena + d.o_V, C * nuv, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
+    const std::vector<int>& perm = b->perms[0];
+    for (int j = 0; j < nuv && rc == SMILI_OK; ++j) {
+      double re, im_;
+      if (b->prec64) {
+        re = reinterpret_cast<double*>(buf.data())[2 * j];
+        im_ = reinterpret_cast<double*>(buf.data())[2 * j + 1];
+      } else {
+        re = reinterpret_cast<float*>(buf.data())[2 * j];
+        im_ = reinterpret_cast<float*>(buf.data())[2 * j + 1];
+      }
+      vreal[perm[j]] = re;
+      vimag[perm[j]] = im_;
+    }
+  }
+  smili_batch_destroy(b);
+  return rc;
+}
+
+int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const double* vreal, const double* vimag,
+                           int nx, int ny, const smili_options* opt, double* img) {
+  if (!u || !v || !vreal || !vimag || !img || nx < 1 || ny < 1 || nuv < 1)
+    return fail(SMILI_ERR_ARG, "invalid nufft arguments");
+  std::vector<double> im;
+  std::vector<int> xi, yi;
+  smili_imaging_args a = bare_args(nuv, u, v, nx, ny, im, xi, yi);
+  smili_batch* b = nullptr;
+  const smili_imaging_args* probs[1] = {&a};
+  int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_T1, nullptr, vreal, vimag, &b);
+  if (rc != SMILI_OK) return rc;
+  rc = run(b, MODE_T1, nullptr);
+  if (rc == SMILI_OK) {
+    const ProbDesc& d = b->descs[0];
+    cudaError_t e = cudaMemcpy(img, b->d_arena + d.o_gchi, sizeof(double) * nx * ny, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
+  }
+  smili_batch_destroy(b);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+"""Non-redundant uv list and signed uv indices for the imaging data terms.
+
+Mirrors ``get_uvlist`` (smili/uvdata/uvtable/tools.py:12-132): the uv points
+of all data terms are stacked in the order fcv, amp, cp (uv12, uv23, uv31),
+ca (uv1..uv4); points with v < 0 are replaced by (-u, -v) and carry sign -1;
+the unique points are sorted lexicographically (u, then v) as ``np.unique``
+sorts complex numbers; each datum gets ``sign * (1 + position in the unique
+list)``.  Closure index arrays come back as (3, Ncp) and (4, Nca) in Fortran
+order, absent tables as 1-element zero dummies, exactly like the reference.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _fold(u: np.ndarray, v: np.ndarray):
+    u = np.array(u, dtype=np.float64, copy=True)
+    v = np.array(v, dtype=np.float64, copy=True)
+    sign = np.ones(u.size, dtype=np.int64)
+    neg = v < 0
+    u[neg] *= -1
+    v[neg] *= -1
+    sign[neg] = -1
+    return u, v, sign
+
+
+def _cols(table, names):
+    return [np.asarray(table[n]).astype(np.float64) for n in names]
+
+
+def get_uvlist(fcvtable=None, amptable=None, bstable=None, catable=None):
+    """Return ``(u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca)``.
+
+    Returns -1 (after printing an error) when no table is given, as the
+    reference does (tools.py:15-18).
+    """
+    if fcvtable is None and amptable is None and bstable is None and catable is None:
+        print("Error: No data are input.")
+        return -1
+    us, vs, ss = [], [], []
+    counts = {"fcv": 0, "amp": 0, "cp": 0, "ca": 0}
+
+    def push(u, v):
+        a, b, s = _fold(u, v)
+        us.append(a)
+        vs.append(b)
+        ss.append(s)
+
+    if fcvtable is not None:
+        u, v = _cols(fcvtable, ["u", "v"])
+        push(u, v)
+        counts["fcv"] = u.size
+    if amptable is not None:
+        u, v = _cols(amptable, ["u", "v"])
+        push(u, v)
+        counts["amp"] = u.size
+    if bstable is not None:
+        cols = _cols(bstable, ["u12", "v12", "u23", "v23", "u31", "v31"])
+        for k in range(3):
+            push(cols[2 * k], cols[2 * k + 1])
+        counts["cp"] = cols[0].size
+    if catable is not None:
+        cols = _cols(catable, ["u1", "v1", "u2", "v2", "u3", "v3", "u4", "v4"])
+        for k in range(4):
+            push(cols[2 * k], cols[2 * k + 1])
+        counts["ca"] = cols[0].size
+
+    ustack = np.concatenate(us)
+    vstack = np.concatenate(vs)
+    sstack = np.concatenate(ss)
+    # lexicographic unique on (u, v): the order numpy uses for complex values
+    order = np.lexsort((vstack, ustack))
+    us_sorted, vs_sorted = ustack[order], vstack[order]
+    new = np.ones(order.size, dtype=bool)
+    new[1:] = (us_sorted[1:] != us_sorted[:-1]) | (vs_sorted[1:] != vs_sorted[:-1])
+    rank = np.cumsum(new) - 1
+    inverse = np.empty(order.size, dtype=np.int64)
+    inverse[order] = rank
+    u = us_sorted[new]
+    v = vs_sorted[new]
+    uvidx = (inverse + 1) * sstack
+
+    nf, na, nc, nq = counts["fcv"], counts["amp"], counts["cp"], counts["ca"]
+    uvidxfcv = uvidx[:nf] if fcvtable is not None else np.zeros(1, dtype=np.int32)
+    uvidxamp = uvidx[nf:nf + na] if amptable is not None else np.zeros(1, dtype=np.int32)
+    if bstable is not None:
+        uvidxcp = uvidx[nf + na:nf + na + 3 * nc].reshape([nc, 3], order="F").transpose()
+    else:
+        uvidxcp = np.zeros([3, 1], dtype=np.int32, order="F")
+    if catable is not None:
+        s0 = nf + na + 3 * nc
+        uvidxca = uvidx[s0:s0 + 4 * nq].reshape([nq, 4], order="F").transpose()
+    else:
+        uvidxca = np.zeros([4, 1], dtype=np.int32, order="F")
+    return (u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca)

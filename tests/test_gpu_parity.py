@@ -1,0 +1,169 @@
+"""CUDA path against the CPU oracle, through the C ABI.
+
+FP64 mode with a tight NUFFT tolerance (1e-12) must match the oracle's exact
+or tight-tolerance result to 1e-9 relative (objective) and 1e-8 relative
+(gradient, max-norm); at the reference's own tolerance (1e-6) both sides are
+1e-6-accurate approximations of the exact transform, so they agree to 1e-5.
+FP32 mode is bounded against the FP64 oracle (see test_calc_cost_fp32_bound).
+L-BFGS-B trajectories agree per iteration: the first 10 iterations to 1e-9
+relative (1e-7 with closure terms), the first 50 to 2e-5 (parallel reductions and atomic spreading change
+the rounding, which the iteration then amplifies slowly).
+"""
+import numpy as np
+import pytest
+
+from conftest import make_kw
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from smili_b200 import _lib
+    return _lib
+
+
+def _rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
+
+
+@pytest.mark.parametrize("nx,ny", [(32, 32), (24, 40), (96, 96)])
+def test_nufft_fwd_matches_dft(oracle, nx, ny):
+    from smili_b200.fortlib import fftlib
+    rng = np.random.default_rng(nx)
+    img = rng.standard_normal((ny, nx))
+    u, v = rng.uniform(-2.5, 2.5, 700), rng.uniform(-2.5, 2.5, 700)
+    ex = oracle.nufft2d2(u, v, img, 0)
+    vr, vi = fftlib.nufft_fwd_real(u, v, img.T, nufft_eps=1e-12)  # (nx, ny) Fortran-order image
+    assert _rel(vr + 1j * vi, ex) < 1e-10
+    vr, vi = fftlib.nufft_fwd_real(u, v, img.T, precision=32, nufft_eps=1e-6)
+    assert _rel(vr + 1j * vi, ex) < 2e-5
+
+
+@pytest.mark.parametrize("nx,ny", [(32, 32), (40, 24)])
+def test_nufft_adj_matches_dft(oracle, nx, ny):
+    from smili_b200.fortlib import fftlib
+    rng = np.random.default_rng(nx + 1)
+    u, v = rng.uniform(-2.5, 2.5, 500), rng.uniform(-2.5, 2.5, 500)
+    c = rng.standard_normal(500) + 1j * rng.standard_normal(500)
+    ex = oracle.nufft2d1(u, v, c, nx, ny, 0).real.reshape(-1)
+    got = fftlib.nufft_adj_real1d(u, v, c.real, c.imag, nx, ny, nufft_eps=1e-12)
+    assert _rel(got, ex) < 1e-10
+
+
+def test_nufft_band_localised_points(oracle):
+    """VLBI-like coverage: all points within a narrow band of the fine grid."""
+    from smili_b200.fortlib import fftlib
+    rng = np.random.default_rng(5)
+    img = rng.random((64, 64))
+    u, v = rng.uniform(-0.3, 0.3, 2000), rng.uniform(-0.25, 0.25, 2000)
+    ex = oracle.nufft2d2(u, v, img, 0)
+    vr, vi = fftlib.nufft_fwd_real(u, v, img.T, nufft_eps=1e-12)
+    assert _rel(vr + 1j * vi, ex) < 1e-10
+
+
+REG_ALL = dict(l1_lambda=1.0, tsv_lambda=1.0, tv_lambda=0.5, kl_lambda=0.1, gs_lambda=0.1,
+               tfd_lambda=1.0, cen_lambda=0.1, sm_lambda=0.1, sm_maj=30.0, sm_min=20.0, sm_phi=30.0)
+
+
+@pytest.mark.parametrize("case", ["fcv_cp_allreg", "amp_cp_ca"])
+def test_calc_cost_fp64_matches_oracle(oracle, crescent32, closure40, case):
+    from smili_b200.fortlib import fftim2d
+    kw = make_kw(crescent32, **REG_ALL) if case == "fcv_cp_allreg" else make_kw(closure40)
+    rng = np.random.default_rng(11)
+    x = kw["iin"] * (1 + 0.3 * rng.random(kw["iin"].size))
+    t_ref, g_ref = oracle.calc_cost(kw, x, eps=1e-12)
+    t_gpu, g_gpu = fftim2d.calc_cost(x, nufft_eps=1e-12, **kw)
+    for k in ["cost", "chisq", "reg", "chisqfcv", "chisqamp", "chisqcp", "chisqca", "l1_cost",
+              "tv_cost", "tsv_cost", "kl_cost", "gs_cost", "tfd_cost", "cen_cost", "sm_cost"]:
+        assert abs(t_gpu[k] - t_ref[k]) <= 1e-9 * max(abs(t_ref[k]), 1e-12), k
+    assert _rel(g_gpu, g_ref) < 1e-8
+    # at the reference's own tolerance (wrapfinufft.f90:8)
+    t6, g6 = fftim2d.calc_cost(x, nufft_eps=1e-6, **kw)
+    t6r, g6r = oracle.calc_cost(kw, x, eps=1e-6)
+    assert abs(t6["cost"] - t6r["cost"]) <= 1e-5 * abs(t6r["cost"])
+    assert _rel(g6, g6r) < 1e-4
+
+
+@pytest.mark.parametrize("case", ["fcv_cp_allreg", "amp_cp_ca"])
+def test_calc_cost_fp32_bound(oracle, crescent32, closure40, case):
+    """FP32 mode (NUFFT tolerance 1e-6) against the exact FP64 objective: the
+    objective within 1e-4 relative, and the gradient error no larger than
+    twice the error that the reference's own FP64 NUFFT at ffteps = 1e-6
+    makes (closure terms divide by |V|^2, so near-null visibilities amplify
+    any transform error in both)."""
+    from smili_b200.fortlib import fftim2d
+    kw = make_kw(crescent32, **REG_ALL) if case == "fcv_cp_allreg" else make_kw(closure40)
+    x = kw["iin"]
+    t_ref, g_ref = oracle.calc_cost(kw, x, eps=1e-12)
+    _, g_ref6 = oracle.calc_cost(kw, x, eps=1e-6)
+    t32, g32 = fftim2d.calc_cost(x, precision=32, nufft_eps=1e-6, **kw)
+    assert abs(t32["cost"] - t_ref["cost"]) <= 1e-4 * abs(t_ref["cost"])
+    assert _rel(g32, g_ref) <= 2.0 * _rel(g_ref6, g_ref) + 1e-4
+
+
+def test_solve_per_iteration_matches_oracle(oracle, crescent32, lib):
+    """First 50 L-BFGS-B iterations: objective per iteration (FP64)."""
+    kw = make_kw(crescent32, niter=50)
+    b = lib.Batch([kw], niter=50, options=lib.make_options(64, 1e-12))
+    b.run()
+    x, terms, _, info = b.fetch(0)
+    tr = b.trace(0, 52)
+    b.close()
+    iout, tref, iref = oracle.imaging(kw, eps=1e-12)
+    trr = iref["trace"]
+    assert info["niter"] == iref["niter"] == 51
+    np.testing.assert_allclose(tr[:10], trr[:10], rtol=1e-9)
+    np.testing.assert_allclose(tr[:50], trr[:50], rtol=2e-5)
+    assert abs(terms["cost"] - tref["cost"]) <= 1e-4 * abs(tref["cost"])
+
+
+def test_solve_closure_terms_matches_oracle(oracle, closure40, lib):
+    kw = make_kw(closure40, niter=40)
+    b = lib.Batch([kw], niter=40, options=lib.make_options(64, 1e-12))
+    b.run()
+    _, terms, _, info = b.fetch(0)
+    tr = b.trace(0, 42)
+    b.close()
+    _, tref, iref = oracle.imaging(kw, eps=1e-12)
+    # closure phases/amplitudes (atan2, log of |V|) amplify rounding more
+    np.testing.assert_allclose(tr[:10], iref["trace"][:10], rtol=1e-7)
+    np.testing.assert_allclose(tr[:30], iref["trace"][:30], rtol=2e-5)
+    assert abs(terms["cost"] - tref["cost"]) <= 1e-4 * abs(tref["cost"])
+
+
+def test_fftim2d_imaging_dropin(oracle, crescent32):
+    from smili_b200.fortlib import fftim2d
+    kw = make_kw(crescent32, niter=30)
+    out = fftim2d.imaging(nufft_eps=1e-12, **kw)
+    assert len(out) == 16 and out[0].shape == (kw["npix"],)
+    iout, tref, _ = oracle.imaging(kw, eps=1e-12)
+    assert abs(out[15] - tref["cost"]) <= 1e-4 * abs(tref["cost"])
+    assert np.abs(out[0] - iout).max() <= 1e-2 * np.abs(iout).max()
+
+
+def test_batched_equals_single(crescent32, closure40, lib):
+    kws = [make_kw(crescent32, niter=20), make_kw(closure40, niter=20), make_kw(crescent32, niter=10)]
+    singles = []
+    for kw in kws:
+        b = lib.Batch([kw], niter=kw["niter"], options=lib.make_options(64, 1e-9))
+        b.run()
+        singles.append(b.fetch(0))
+        b.close()
+    b = lib.Batch(kws, niter=[k["niter"] for k in kws], options=lib.make_options(64, 1e-9))
+    b.run()
+    for p, s in enumerate(singles):
+        x, t, _, info = b.fetch(p)
+        assert info["niter"] == s[3]["niter"]
+        assert abs(t["cost"] - s[1]["cost"]) <= 1e-9 * abs(s[1]["cost"])
+    b.close()
+
+
+def test_invalid_inputs_raise(crescent32, lib):
+    kw = make_kw(crescent32, niter=5)
+    bad = dict(kw)
+    bad["varfcv"] = kw["varfcv"].copy()
+    bad["varfcv"][3] = 0.0
+    with pytest.raises(lib.SmiliError) as e:
+        lib.Batch([bad], niter=5)
+    assert e.value.code == -2
