@@ -98,14 +98,22 @@ typedef struct smili_batch smili_batch;
 int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const int* niter,
                        int nonneg, int m, double factr, double pgtol, const smili_options* opt,
                        smili_batch** out);
-/* Solve (or, with fg_only != 0, evaluate calc_cost once) every problem on the
- * device; kernel_ms (optional) receives the device time of the launch. */
+/* Solve (fg_only = 0) or evaluate calc_cost once (fg_only = 1) for every
+ * problem on the device; fg_only = 2 only times 1000 group barriers (a
+ * diagnostic).  kernel_ms (optional) receives the device time of the launch. */
 int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms);
 int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double* grad,
                       smili_solve_info* info);
 /* Cost recorded at each completed iteration of problem p (NaN where absent). */
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len);
 void smili_batch_destroy(smili_batch* b);
+/* Stage profiler (no reference counterpart): with enable != 0 the next runs
+ * accumulate the device time of each solver stage of the first CTA group;
+ * stage_ns (optional, len entries) receives the last accumulated values in
+ * the order F1..F8 (transform and data stages), L-BFGS-B bookkeeping,
+ * Cauchy point, formk, subspace minimisation, line-search start, set-up,
+ * other, evaluation count. */
+int smili_batch_profile(smili_batch* b, int enable, double* stage_ns, int len);
 
 /* NUFFTs of the imaging path with the reference's conventions (sign "+",
  * modes -N/2..(N-1)/2 at pixels 1..N): fortlib.fftlib.nufft_fwd_real

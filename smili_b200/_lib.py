@@ -67,7 +67,10 @@ TASK_CONV, TASK_ABNORMAL, TASK_STOP, TASK_ERROR = 3, 4, 5, 6
 
 EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "smili_batch_run",
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
-           "smili_nufft_adj_real1d", "smili_last_error", "smili_version"]
+           "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile"]
+STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
+          "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
+          "c_gather", "c_sort", "c_scan", "c_rounds"]
 
 
 def lib():
@@ -89,6 +92,7 @@ def lib():
         L.smili_batch_trace.argtypes = [vp, C.c_int, dp, C.c_int]
         L.smili_batch_destroy.argtypes = [vp]
         L.smili_batch_destroy.restype = None
+        L.smili_batch_profile.argtypes = [vp, C.c_int, dp, C.c_int]
         L.smili_nufft_fwd_real.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp, vp, dp, dp]
         L.smili_nufft_adj_real1d.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, vp, dp]
         _lib = L
@@ -174,9 +178,11 @@ class Batch:
         self.n = n
 
     def run(self, fg_only=False):
-        """Run on the device; returns the launch's device time in ms."""
+        """Run on the device; returns the launch's device time in ms.
+        fg_only: False solve, True one evaluation, 2 time 1000 group barriers."""
         ms = C.c_float(0.0)
-        check(lib().smili_batch_run(self.h, int(bool(fg_only)), C.byref(ms)))
+        mode = 2 if fg_only == 2 else int(bool(fg_only))
+        check(lib().smili_batch_run(self.h, mode, C.byref(ms)))
         return float(ms.value)
 
     def fetch(self, p):
@@ -187,6 +193,18 @@ class Batch:
         check(lib().smili_batch_fetch(self.h, p, dptr(x), dptr(terms), dptr(g), C.byref(info)))
         return x, dict(zip(TERM_NAMES, terms)), g, {"task": info.task, "niter": info.niter,
                                                      "nfg": info.nfg, "error": info.error}
+
+    def profile(self, enable=True):
+        check(lib().smili_batch_profile(self.h, int(bool(enable)), None, 0))
+
+    def stage_times(self):
+        """Accumulated stage times (ms) of the last profiled run, and the FG count."""
+        t = np.zeros(len(STAGES))
+        check(lib().smili_batch_profile(self.h, 1, dptr(t), len(STAGES)))
+        out = {k: t[i] / 1e6 for i, k in enumerate(STAGES)}
+        out["n_fg"] = int(t[STAGES.index("n_fg")])
+        out["c_rounds"] = int(t[STAGES.index("c_rounds")])
+        return out
 
     def trace(self, p, length):
         t = np.zeros(length)

@@ -215,3 +215,37 @@ __device__ void block_reduce_arr(const double* v, const unsigned char* ops, int 
   }
   __syncthreads();
 }
+
+// ---------------------------------------------------------------------------
+// Stage profiler: CTA 0 (thread 0) accumulates the time between consecutive
+// marks into acc[stage] (nanoseconds, from %globaltimer).  Off when acc is 0.
+// ---------------------------------------------------------------------------
+enum {
+  PR_F1 = 0, PR_F2, PR_F3, PR_F4, PR_F5, PR_F6, PR_F7, PR_F8, PR_LB_POST, PR_CAUCHY, PR_FORMK,
+  PR_SUBSM, PR_LNSRCH, PR_INIT, PR_OTHER, PR_COUNT, PR_C_SEL, PR_C_GATHER, PR_C_SORT, PR_C_SCAN,
+  PR_C_ROUNDS, PR_NSTAGE
+};
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+struct Prof {
+  unsigned long long* acc;
+  unsigned long long t;
+  __device__ void start() {
+    if (acc) t = gtimer();
+  }
+  __device__ void mark(int st) {
+    if (acc) {
+      const unsigned long long now = gtimer();
+      acc[st] += now - t;
+      t = now;
+    }
+  }
+  __device__ void count(int st) {
+    if (acc) acc[st] += 1;
+  }
+};

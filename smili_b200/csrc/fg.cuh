@@ -44,7 +44,8 @@ struct FgCtx {
   char* base;
   cpx<R>* sbuf;   // shared: 2 * SMEM_CPX complex values
   cpx<R>* swork;
-  int smem_cpx;   // capacity of each of the two buffers (complex elements)
+  int smem_cpx;   // capacity of each of the two FFT buffers (complex elements)
+  int dyn_cpx;    // capacity of the whole dynamic shared region (complex elements)
 };
 
 // Running compensated sum (TwoSum) used for the chi-square terms
@@ -173,10 +174,22 @@ __device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
   const ProbDesc& P = *c.P;
   const R* xu = at<R>(c.base, P.o_u);
   const R* xv = at<R>(c.base, P.o_v);
-  const cpx<R>* bandA = at<cpx<R>>(c.base, P.o_bandA);
+  const cpx<R>* gband = at<cpx<R>>(c.base, P.o_bandA);
   cpx<R>* V = at<cpx<R>>(c.base, P.o_V);
   const int w = P.w;
   const R beta = (R)P.beta;
+  const int ncell = P.b1n * P.b2n;
+  // the band is re-read w*w times per point: stage it in shared memory
+  const bool staged = ncell <= c.dyn_cpx;
+  const cpx<R>* bandA = gband;
+  if (staged) {
+    // only CTAs that own points load the band
+    if (g.rank * SMILI_THREADS < P.nuv) {
+      for (int i = threadIdx.x; i < ncell; i += blockDim.x) c.sbuf[i] = gband[i];
+      __syncthreads();
+      bandA = c.sbuf;
+    }
+  }
   for (int j = g.rank * SMILI_THREADS + threadIdx.x; j < P.nuv; j += g.G * SMILI_THREADS) {
     int l1, l2;
     R k1[SMILI_MAXW], k2[SMILI_MAXW];
@@ -201,6 +214,7 @@ __device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
     }
     V[j] = cmk(ar, ai);
   }
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -299,41 +313,127 @@ __device__ __forceinline__ void atomic_add_r(double* p, double v) { atomicAdd(p,
 __device__ __forceinline__ void atomic_add_r(float* p, float v) { atomicAdd(p, v); }
 
 template <typename R>
+__device__ __forceinline__ R warp_sum(R v) {
+  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+  return v;
+}
+
+// Subproblem spreading.  The bin-sorted points are cut into work items of
+// at most 128 points that share one 8x8 bin of the band.  A warp owns an item
+// and a private (8+w-1)^2 subgrid in shared memory: for every point the
+// lanes cover the w*w taps (all lanes hit different cells, and consecutive
+// points are ordered by __syncwarp), so the inner loop needs no atomics.  The
+// finished subgrid is added to the CTA's band copy (shared atomics, only the
+// overlapping halos collide) and the CTA's band to the global band at the end.
+#define SMILI_BIN 8
+template <typename R>
 __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
   const ProbDesc& P = *c.P;
   const R* xu = at<R>(c.base, P.o_u);
   const R* xv = at<R>(c.base, P.o_v);
   const int* off = at<int>(c.base, P.o_csr_off);
   const int* ent = at<int>(c.base, P.o_csr_ent);
+  const int4* items = at<int4>(c.base, P.o_items);
   const cpx<R>* contrib = at<cpx<R>>(c.base, P.o_contrib);
-  R* band = at<R>(c.base, P.o_bandC);
-  const int w = P.w;
+  R* gband = at<R>(c.base, P.o_bandC);
+  const int w = P.w, ww = P.w * P.w;
+  const int SG = SMILI_BIN + w - 1;  // subgrid side
   const R beta = (R)P.beta;
-  for (int j = g.rank * SMILI_THREADS + threadIdx.x; j < P.nuv; j += g.G * SMILI_THREADS) {
-    R cre = 0, cim = 0;
-    for (int e = off[j]; e < off[j + 1]; ++e) {
-      const cpx<R> q = contrib[ent[e]];
-      cre += q.x;
-      cim += q.y;
-    }
-    cim = -cim;  // c = Vresre - i Vresim
-    int l1, l2;
-    R k1[SMILI_MAXW], k2[SMILI_MAXW];
-    taps(xu[j], w, beta, l1, k1);
-    taps(xv[j], w, beta, l2, k2);
-    const int c1 = imod(l1 - P.b1s, P.nf1), c2 = imod(l2 - P.b2s, P.nf2);
-    for (int b = 0; b < w; ++b) {
-      int rw = c2 + b;
-      if (rw >= P.nf2) rw -= P.nf2;
-      R* row = band + 2 * (size_t)rw * P.b1n;
-      const R wr = k2[b] * cre, wi = k2[b] * cim;
-      for (int a = 0; a < w; ++a) {
-        int cl = c1 + a;
-        if (cl >= P.nf1) cl -= P.nf1;
-        atomic_add_r(row + 2 * cl, k1[a] * wr);
-        atomic_add_r(row + 2 * cl + 1, k1[a] * wi);
+  const R half = (R)0.5 * (R)w, inv = (R)1 / half;
+  const int ncell = P.b1n * P.b2n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // shared memory: [nw][SG*SG] complex subgrids, [nw][PB][2w] kernel weights,
+  // then (if it fits) a private copy of the band.  PB = points prepared per
+  // phase, the largest of 32/16/8 that fits.
+  const size_t sub_b = (size_t)nw * SG * SG * sizeof(cpx<R>);
+  const size_t dyn_b = (size_t)c.dyn_cpx * sizeof(cpx<R>);
+  int PB = 32;
+  while (PB > 8 && sub_b + (size_t)nw * PB * 2 * w * sizeof(R) > dyn_b) PB >>= 1;
+  const size_t wt_b = ((size_t)nw * PB * 2 * w * sizeof(R) + 15) / 16 * 16;
+  cpx<R>* sub = c.sbuf + (size_t)warp * SG * SG;
+  R* wtab = reinterpret_cast<R*>(reinterpret_cast<char*>(c.sbuf) + sub_b) + (size_t)warp * PB * 2 * w;
+  cpx<R>* sband = reinterpret_cast<cpx<R>*>(reinterpret_cast<char*>(c.sbuf) + sub_b + wt_b);
+  const bool staged = sub_b + wt_b + (size_t)ncell * sizeof(cpx<R>) <= dyn_b;
+  R* band = staged ? reinterpret_cast<R*>(sband) : gband;
+  if (staged) {
+    for (int i = threadIdx.x; i < ncell; i += blockDim.x) sband[i] = cmk<R>(0, 0);
+    __syncthreads();
+  }
+  const int ra = lane % w, rb = lane / w;
+  const int gw = g.rank * nw + warp, nwt = g.G * nw;
+  for (int it = gw; it < P.nitems; it += nwt) {
+    const int4 item = items[it];
+    for (int i = lane; i < SG * SG; i += 32) sub[i] = cmk<R>(0, 0);
+    for (int jb = item.x; jb < item.y; jb += PB) {
+      // phase 1: lanes < PB prepare one point each (slots, cell, kernel weights)
+      const int jl = jb + lane;
+      R cre_l = 0, cim_l = 0;
+      int cell_l = 0;
+      if (lane < PB && jl < item.y) {
+        const int e1 = off[jl + 1];
+        for (int e = off[jl]; e < e1; ++e) {
+          const cpx<R> q = contrib[ent[e]];
+          cre_l += q.x;
+          cim_l += q.y;
+        }
+        const R xi1 = xu[jl], xi2 = xv[jl];
+        const int l1 = (int)ceil(xi1 - half), l2 = (int)ceil(xi2 - half);
+        R* wr = wtab + lane * 2 * w;
+        for (int q = 0; q < w; ++q) {
+          wr[q] = es_kernel(((R)(l1 + q) - xi1) * inv, beta);
+          wr[w + q] = es_kernel(((R)(l2 + q) - xi2) * inv, beta);
+        }
+        // position inside the subgrid (item.z, item.w = subgrid origin row, col)
+        const int lr = imod(l2 - P.b2s, P.nf2) - item.z, lc = imod(l1 - P.b1s, P.nf1) - item.w;
+        cell_l = lr * SG + lc;
+      }
+      __syncwarp();
+      // phase 2: the lanes cover the taps of one point at a time
+      const int np = min(PB, item.y - jb);
+      for (int p = 0; p < np; ++p) {
+        const R cre = __shfl_sync(0xffffffffu, cre_l, p);
+        const R cim = -__shfl_sync(0xffffffffu, cim_l, p);  // c = Vresre - i Vresim
+        const int cell0 = __shfl_sync(0xffffffffu, cell_l, p);
+        const R* wr = wtab + p * 2 * w;
+        int a = ra, b = rb;
+        for (int t0 = 0; t0 < ww; t0 += 32) {
+          if (t0 + lane < ww) {
+            cpx<R>& cell = sub[cell0 + b * SG + a];
+            const R wt = wr[a] * wr[w + b];
+            cell.x += wt * cre;
+            cell.y += wt * cim;
+          }
+          a += 32 % w;
+          b += 32 / w;
+          if (a >= w) {
+            a -= w;
+            b += 1;
+          }
+        }
+        __syncwarp();
       }
     }
+    // add the subgrid to the band (rows/cols wrap only for a full-grid band)
+    for (int i = lane; i < SG * SG; i += 32) {
+      const cpx<R> v = sub[i];
+      if (v.x == (R)0 && v.y == (R)0) continue;
+      int rw = item.z + i / SG, cl = item.w + i % SG;
+      if (rw >= P.nf2) rw -= P.nf2;
+      if (cl >= P.nf1) cl -= P.nf1;
+      if (rw >= P.b2n || cl >= P.b1n) continue;  // beyond the band: only zero taps land here
+      R* dst = band + 2 * ((size_t)rw * P.b1n + cl);
+      atomic_add_r(dst, v.x);
+      atomic_add_r(dst + 1, v.y);
+    }
+    __syncwarp();
+  }
+  if (staged) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * ncell; i += blockDim.x) {
+      const R vv = band[i];
+      if (vv != (R)0) atomic_add_r(gband + i, vv);
+    }
+    __syncthreads();
   }
 }
 

@@ -38,7 +38,7 @@ struct ProbDesc {
   int nonneg, m, niter, prec64;
   int has_l1, has_tv, has_tsv, has_kl, has_gs, has_tfd, has_cen, has_sm;
   int windowed;            // 1 when the pixel set is not the full nx*ny grid
-  int pad0;
+  int nitems;              // spreading work items (<= 128 points of one 8x8 bin)
   // scalars
   double beta;
   double wfcv, wamp, wcp, wca;       // normalised data weights (w / wtotal)
@@ -55,10 +55,12 @@ struct ProbDesc {
   int64_t o_didx;                       // per slot: 0-based uv index (sorted order)
   int64_t o_dsgn;                       // per slot: sign (+1 / -1) as int8
   int64_t o_csr_off, o_csr_ent;         // uv point -> contribution slots
+  int64_t o_items;                      // int4 work items: start, end, row0, col0
   int64_t o_tmpA, o_bandA, o_V, o_contrib, o_bandC, o_tmpC, o_gchi;
   int64_t o_part;                       // FG partial sums [npart_ctas][SMILI_NPART] (double)
   // optimiser (double precision)
   int64_t o_x, o_g, o_z, o_r, o_d, o_t, o_xp, o_ws, o_wy, o_iwh, o_free, o_bkey;
+  int64_t o_sbk, o_sbi, o_hist;         // bucketed breakpoints, bucket counts/cursors
   int64_t o_cand, o_lred, o_state;
   int64_t o_trace;                      // cost at each NEW_X (double[niter+2])
   int64_t o_out;                        // results: terms[15], counters

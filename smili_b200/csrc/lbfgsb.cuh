@@ -46,6 +46,7 @@ struct LbCtx {
   unsigned char* ops;
   double* scratch;
   char* dyn;      // shared scratch (the FFT buffers)
+  Prof* prof;
 };
 
 // ---------------------------------------------------------------------------
@@ -391,66 +392,162 @@ __device__ void block_scan_incl(double* vals, int V, double* wtot /* shared [WAR
   __syncthreads();
 }
 
-// Sequential-order scan of the breakpoints by one CTA (the group leader).
-// Inputs: c.bkey (breakpoint keys, ~0 for none), c.d, columns; f1_0, p_0 in
-// pv; nbreak; bnded.  Writes the CR_* results.
-__device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak, int bnded) {
+// Breakpoint bucketing (all CTAs of the group).  Keys are the IEEE bits of
+// the breakpoint times t > 0, which order like the times; bucket =
+// (key - kmin) >> shift, with the shift chosen so that the keys span at most
+// SMILI_NBUCKET buckets.  sbk/sbi receive the breakpoints grouped by bucket in
+// increasing bucket order (unordered inside a bucket); hist the bucket counts.
+#define SMILI_NBUCKET 4096
+
+__device__ __forceinline__ int bucket_of(unsigned long long k, unsigned long long kmin, int shift) {
+  const unsigned long long q = (k - kmin) >> shift;
+  return q < (unsigned long long)SMILI_NBUCKET ? (int)q : SMILI_NBUCKET - 1;
+}
+
+// Select the next batch (<= SMILI_KC elements, the smallest composites above
+// lo_key) from the unordered range [r0, r1) of the bucketed arrays into cand,
+// by radix selection on 12-bit digits of the 96-bit composite (key, index).
+// Used for a bucket that holds more than SMILI_KC breakpoints.
+__device__ int select_from_range(LbCtx& c, const unsigned long long* sbk, const int* sbi, int r0,
+                                 int r1, u128 lo_key, u128* cand, unsigned* hist) {
+  __shared__ int cnt_s, vstar_s, cum_s;
+  u128 prefix = 0;
+  int level = 0, budget = SMILI_KC;
+  u128 sel_hi = ~(u128)0;
+  bool have_hi = false;
+  while (true) {
+    const int shift = 96 - 12 * (level + 1);
+    for (int i = threadIdx.x; i < 4096; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+      const u128 ck = comp_key(sbk[i], sbi[i]);
+      if (ck <= lo_key) continue;
+      if (level > 0 && (ck >> (96 - 12 * level)) != prefix) continue;
+      atomicAdd(&hist[(unsigned)((ck >> shift) & 0xfffu)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int cum = 0, vstar = -1;
+      for (int b = 0; b < 4096; ++b) {
+        if (cum + (int)hist[b] > budget) {
+          vstar = b;
+          break;
+        }
+        cum += hist[b];
+      }
+      vstar_s = vstar;
+      cum_s = cum;
+    }
+    __syncthreads();
+    const int vstar = vstar_s, cum = cum_s;
+    if (vstar < 0) {
+      if (level > 0) {
+        sel_hi = (prefix + 1) << (96 - 12 * level);
+        have_hi = true;
+      }
+      break;
+    }
+    const u128 np = (prefix << 12) | (u128)vstar;
+    if (cum == budget || (cum > 0 && (4 * cum >= budget || level == 7))) {
+      sel_hi = np << shift;
+      have_hi = true;
+      break;
+    }
+    budget -= cum;
+    prefix = np;
+    ++level;
+  }
+  if (threadIdx.x == 0) cnt_s = 0;
+  __syncthreads();
+  for (int i0 = r0; i0 < r1; i0 += blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    bool take = false;
+    u128 ck = 0;
+    if (i < r1) {
+      ck = comp_key(sbk[i], sbi[i]);
+      take = ck > lo_key && !(have_hi && ck >= sel_hi);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, take);
+    if (bal) {
+      const int lane = threadIdx.x & 31;
+      int base = 0;
+      if (lane == __ffs(bal) - 1) base = atomicAdd(&cnt_s, __popc(bal));
+      base = __shfl_sync(0xffffffffu, base, __ffs(bal) - 1);
+      const int pos = base + __popc(bal & ((1u << lane) - 1));
+      if (take && pos < SMILI_KC) cand[pos] = ck;
+    }
+  }
+  __syncthreads();
+  const int cnt = min(cnt_s, SMILI_KC);
+  __syncthreads();
+  return cnt;
+}
+
+// Sequential-order scan of the bucketed breakpoints by one CTA (the group
+// leader): batches of whole buckets (<= SMILI_KC elements) are sorted by
+// (t, index) and swept with the closed-form piecewise quadratic.  Writes the
+// CR_* results.
+__device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak, int bnded,
+                            const unsigned long long* sbk, const int* sbi, const int* ghist) {
   LbState& S = *c.S;
   const int m = c.m, col = S.col, col2 = 2 * col, n = c.n;
   const double theta = S.theta;
   // shared layout inside dyn
   u128* cand = reinterpret_cast<u128*>(c.dyn);                        // SMILI_KC
-  unsigned* hist = reinterpret_cast<unsigned*>(cand + SMILI_KC);      // 4096
-  double* wtot = reinterpret_cast<double*>(hist + 4096);              // WARPS*32
+  unsigned* hist = reinterpret_cast<unsigned*>(cand + SMILI_KC);      // 4096 (bucket counts)
+  unsigned* hist2 = hist + SMILI_NBUCKET;                             // 4096 (fallback)
+  double* wtot = reinterpret_cast<double*>(hist2 + 4096);             // WARPS*32
   double* dtm_s = wtot + SMILI_WARPS * 32;                            // THREADS
   double* t_s = dtm_s + SMILI_THREADS;                                // THREADS
-  double* st = t_s + SMILI_THREADS;                                   // carried state
-  // st: [0]=D [1]=tprev [2]=dtm_cur [3]=kdone [4]=found [5..5+2m)=P [..+2m)=Q
-  //     [..] boundary hi, lo bits stored separately below
-  __shared__ unsigned long long bnd_hi_s, bnd_lo_s, sel_hi_hi, sel_hi_lo;
-  __shared__ int cnt_s, e_star_s;
-  __shared__ double res_s[4 + 2 * SMILI_MAXM_DEV];
+  double* Mm = t_s + SMILI_THREADS;                                   // dense M (2col)^2
+  double* st = Mm + 4 * SMILI_MAXM_DEV * SMILI_MAXM_DEV;              // carried state
+  // st: [0]=D [1]=tprev [2]=dtm_cur [3..] unused [5..5+2m)=P [..+2m)=Q
+  __shared__ unsigned long long bnd_hi_s, bnd_lo_s;
+  __shared__ int e_star_s, info_s;
+  __shared__ double f2org_s;
   double* Pst = st + 5;
   double* Qst = Pst + 2 * SMILI_MAXM_DEV;
+  Prof& pf = *c.prof;
+  double* lr = c.lred;
 
+  // dense middle matrix: column j = M e_j
+  if (threadIdx.x == 0) info_s = 0;
+  __syncthreads();
+  if (threadIdx.x < col2) {
+    double e[2 * SMILI_MAXM_DEV], mc[2 * SMILI_MAXM_DEV];
+    for (int k = 0; k < col2; ++k) e[k] = (k == (int)threadIdx.x) ? 1.0 : 0.0;
+    if (d_bmv(S, m, col, e, mc)) info_s = -1;
+    for (int k = 0; k < col2; ++k) Mm[k * col2 + threadIdx.x] = mc[k];
+  }
+  for (int i = threadIdx.x; i < SMILI_NBUCKET; i += blockDim.x) hist[i] = (unsigned)ghist[i];
+  __syncthreads();
+  if (info_s) {  // singular middle matrix (bmv failure)
+    if (threadIdx.x == 0) lr[CR_INFO] = -1;
+    __syncthreads();
+    return;
+  }
   if (threadIdx.x == 0) {
-    double v[2 * SMILI_MAXM_DEV];
     double f2 = -theta * f1_0;
     const double f2_org = f2;
-    int info = 0;
     if (col > 0) {
-      info = d_bmv(S, m, col, p0, v);
       double s = 0;
-      for (int j = 0; j < col2; ++j) s += v[j] * p0[j];
+      for (int i = 0; i < col2; ++i)
+        for (int j = 0; j < col2; ++j) s += p0[i] * Mm[i * col2 + j] * p0[j];
       f2 -= s;
     }
     st[0] = -f1_0;
     st[1] = 0.0;
     st[2] = -f1_0 / f2;
-    st[3] = 0;
-    st[4] = info ? -1 : 0;
     for (int j = 0; j < col2; ++j) {
       Pst[j] = p0[j];
       Qst[j] = 0.0;
     }
-    res_s[0] = f2_org;
+    f2org_s = f2_org;
     bnd_hi_s = 0;
     bnd_lo_s = 0;
   }
   __syncthreads();
-  const double f2_org = res_s[0];
-  double* lr = c.lred;
-  if (st[4] < 0) {  // bmv failure (singular middle matrix)
-    if (threadIdx.x == 0) lr[CR_INFO] = -1;
-    __syncthreads();
-    return;
-  }
-  // pointers of the logical columns
-  int pj[SMILI_MAXM_DEV];
-  for (int j = 0; j < col; ++j) pj[j] = lptr(S, m, j);
-
-  int kdone = 0;
-  const int V = 1 + 2 * col2;
+  const double f2_org = f2org_s;
   if (nbreak == 0) {  // GCP in the first segment (lbfgsb.f:1433, label 888)
     if (threadIdx.x == 0) {
       double dtm = st[2];
@@ -466,80 +563,36 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
     __syncthreads();
     return;
   }
+  int pj[SMILI_MAXM_DEV];
+  for (int j = 0; j < col; ++j) pj[j] = lptr(S, m, j);
+  const int V = 1 + 2 * col2;
+  int kdone = 0, pos = 0, bucket = 0;
+  // state of an oversized bucket being consumed by radix selection
+  int big_r0 = -1, big_r1 = -1;
   while (true) {
-    // ---------------- selection of the next batch (radix select) ----------
+    // ---------------- next batch ----------------
+    int cnt = 0;
     const u128 lo_key = ((u128)bnd_hi_s << 64) | (u128)bnd_lo_s;
-    u128 prefix = 0;
-    int level = 0, budget = SMILI_KC;
-    u128 sel_hi = ~(u128)0;  // exclusive upper bound of the batch
-    bool have_hi = false;
-    while (true) {
-      const int shift = 96 - 12 * (level + 1);
-      for (int i = threadIdx.x; i < 4096; i += blockDim.x) hist[i] = 0;
-      __syncthreads();
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const unsigned long long k = c.bkey[i];
-        if (k == ~0ULL) continue;
-        const u128 ck = comp_key(k, i);
-        if (ck <= lo_key) continue;
-        if (level > 0 && (ck >> (96 - 12 * level)) != prefix) continue;
-        atomicAdd(&hist[(unsigned)((ck >> shift) & 0xfffu)], 1u);
+    if (big_r0 < 0) {
+      while (bucket < SMILI_NBUCKET && hist[bucket] == 0) ++bucket;
+      if (bucket < SMILI_NBUCKET && (int)hist[bucket] > SMILI_KC) {
+        big_r0 = pos;
+        big_r1 = pos + (int)hist[bucket];
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int cum = 0, vstar = -1;
-        for (int b = 0; b < 4096; ++b) {
-          if (cum + (int)hist[b] > budget) {
-            vstar = b;
-            break;
-          }
-          cum += hist[b];
-        }
-        if (vstar < 0) {
-          // everything under this prefix fits
-          e_star_s = -1;
-          cnt_s = cum;
-        } else {
-          e_star_s = vstar;
-          cnt_s = cum;
-        }
-      }
-      __syncthreads();
-      const int vstar = e_star_s, cum = cnt_s;
-      if (vstar < 0) {
-        if (level > 0) {
-          sel_hi = (prefix + 1) << (96 - 12 * level);
-          have_hi = true;
-        }
-        break;
-      }
-      const u128 np = (prefix << 12) | (u128)vstar;
-      // bins below vstar are taken; stop when they fill the batch well
-      // enough, else refine inside bin vstar with the remaining budget.  At
-      // the last digit every bin holds one composite key, so this ends.
-      if (cum == budget || (cum > 0 && (4 * cum >= budget || level == 7))) {
-        sel_hi = np << shift;
-        have_hi = true;
-        break;
-      }
-      budget -= cum;
-      prefix = np;
-      ++level;
     }
-    // ---------------- gather the batch ----------------
-    if (threadIdx.x == 0) cnt_s = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const unsigned long long k = c.bkey[i];
-      if (k == ~0ULL) continue;
-      const u128 ck = comp_key(k, i);
-      if (ck <= lo_key) continue;
-      if (have_hi && ck >= sel_hi) continue;
-      const int pos = atomicAdd(&cnt_s, 1);
-      if (pos < SMILI_KC) cand[pos] = ck;
+    if (big_r0 >= 0) {
+      cnt = select_from_range(c, sbk, sbi, big_r0, big_r1, lo_key, cand, hist2);
+    } else {
+      int b2 = bucket, tot = 0;
+      while (b2 < SMILI_NBUCKET && tot + (int)hist[b2] <= SMILI_KC) tot += hist[b2++];
+      for (int i = threadIdx.x; i < tot; i += blockDim.x) cand[i] = comp_key(sbk[pos + i], sbi[pos + i]);
+      cnt = tot;
+      pos += tot;
+      bucket = b2;
     }
     __syncthreads();
-    const int cnt = min(cnt_s, SMILI_KC);
+    pf.mark(PR_C_SEL);
+    pf.count(PR_C_ROUNDS);
     int np2 = 1;
     while (np2 < cnt) np2 <<= 1;
     for (int i = cnt + threadIdx.x; i < np2; i += blockDim.x) cand[i] = ~(u128)0;
@@ -561,6 +614,7 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
         __syncthreads();
       }
     }
+    pf.mark(PR_C_SORT);
     // ---------------- scan in chunks of THREADS ----------------
     bool finished = false;
     for (int base = 0; base < cnt; base += SMILI_THREADS) {
@@ -597,14 +651,12 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
           Pk[j] = Pst[j] - vals[1 + j];
           ck_[j] = te * Pk[j] + (Qst[j] + vals[1 + col2 + j]);
         }
-        double Mp[2 * SMILI_MAXM_DEV];
         double cMp = 0.0, pMp = 0.0;
-        if (col > 0) {
-          d_bmv(S, m, col, Pk, Mp);
-          for (int j = 0; j < col2; ++j) {
-            cMp += ck_[j] * Mp[j];
-            pMp += Pk[j] * Mp[j];
-          }
+        for (int i = 0; i < col2; ++i) {
+          double mp = 0.0;
+          for (int j = 0; j < col2; ++j) mp += Mm[i * col2 + j] * Pk[j];
+          cMp += ck_[i] * mp;
+          pMp += Pk[i] * mp;
         }
         const double f1 = -Dk + theta * te * Dk - cMp;
         double f2 = theta * Dk - pMp;
@@ -705,7 +757,13 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
         break;
       }
     }
+    pf.mark(PR_C_SCAN);
     if (finished) break;
+    if (big_r0 >= 0 && kdone >= big_r1) {  // the oversized bucket is consumed
+      pos = big_r1;
+      ++bucket;
+      big_r0 = big_r1 = -1;
+    }
   }
   __syncthreads();
 }
@@ -716,6 +774,9 @@ __device__ int lb_cauchy(LbCtx& c) {
   const ProbDesc& P = *c.P;
   const int m = c.m, n = c.n, col = S.col, col2 = 2 * col;
   const bool nonneg = P.nonneg;
+  unsigned long long* sbk = at<unsigned long long>(c.base, P.o_sbk);
+  int* sbi = at<int>(c.base, P.o_sbi);
+  int* ghist = at<int>(c.base, P.o_hist);  // [NBUCKET] counts, [NBUCKET] cursors
   if (S.sbgnrm <= 0.0) {
     // GCP = X (lbfgsb.f:1318-1322): z = x, iwhere untouched
     for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) c.z[i] = c.x[i];
@@ -724,9 +785,13 @@ __device__ int lb_cauchy(LbCtx& c) {
     int pj[SMILI_MAXM_DEV];
     for (int j = 0; j < col; ++j) pj[j] = lptr(S, m, j);
     // acc: [0]=f1 [1..2col]=p [2col+1]=nbreak [2col+2]=nfree_nb [2col+3]=notbnded
-    const int K = col2 + 4;
-    double acc[2 * SMILI_MAXM_DEV + 4];
+    //      [2col+4]=tmin [2col+5]=tmax
+    const int K = col2 + 6;
+    double acc[2 * SMILI_MAXM_DEV + 6];
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    acc[col2 + 4] = 1.0e308;
+    for (int i = c.g->rank * SMILI_THREADS + threadIdx.x; i < 2 * SMILI_NBUCKET; i += c.g->G * SMILI_THREADS)
+      ghist[i] = 0;
     for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
       const double neggi = -c.gv[i];
       int iw = c.iwh[i];
@@ -753,8 +818,11 @@ __device__ int lb_cauchy(LbCtx& c) {
           acc[1 + col + j] += c.ws[(size_t)pj[j] * n + i] * neggi;
         }
         if (nonneg && neggi < 0.0) {
+          const double tb = tl / (-neggi);
           acc[col2 + 1] += 1.0;
-          key = (unsigned long long)__double_as_longlong(tl / (-neggi));
+          acc[col2 + 4] = fmin(acc[col2 + 4], tb);
+          acc[col2 + 5] = fmax(acc[col2 + 5], tb);
+          key = (unsigned long long)__double_as_longlong(tb);
         } else {
           acc[col2 + 2] += 1.0;
           if (fabs(neggi) > 0.0) acc[col2 + 3] = 1.0;
@@ -762,7 +830,8 @@ __device__ int lb_cauchy(LbCtx& c) {
       }
       c.bkey[i] = key;
     }
-    for (int k = threadIdx.x; k < K; k += blockDim.x) c.ops[k] = (k == col2 + 3) ? RED_MAX : RED_SUM;
+    for (int k = threadIdx.x; k < K; k += blockDim.x)
+      c.ops[k] = (k == col2 + 3 || k == col2 + 5) ? RED_MAX : (k == col2 + 4 ? RED_MIN : RED_SUM);
     __syncthreads();
     if (!lb_reduce(c, acc, K)) return -2;
     const double f1 = c.red[0];
@@ -771,6 +840,8 @@ __device__ int lb_cauchy(LbCtx& c) {
     const int nbreak = (int)c.red[col2 + 1];
     const int nfree_nb = (int)c.red[col2 + 2];
     const int bnded = c.red[col2 + 3] > 0.5 ? 0 : 1;
+    const unsigned long long kmin = (unsigned long long)__double_as_longlong(c.red[col2 + 4]);
+    const unsigned long long kmax = (unsigned long long)__double_as_longlong(c.red[col2 + 5]);
     if (S.theta != 1.0)
       for (int j = 0; j < col; ++j) p[col + j] *= S.theta;
     __syncthreads();
@@ -778,7 +849,54 @@ __device__ int lb_cauchy(LbCtx& c) {
       for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) c.z[i] = c.x[i];
       if (threadIdx.x == 0 && c.g->rank == 0) c.lred[CR_MODE] = CM_XCP_IS_X;
     } else {
-      if (c.g->rank == 0) cauchy_scan(c, f1, p, nbreak, bnded);
+      if (nbreak > 0) {
+        // bucket the breakpoints: histogram, then scatter in bucket order
+        int shift = 0;
+        while (shift < 63 && ((kmax - kmin) >> shift) >= (unsigned long long)SMILI_NBUCKET) ++shift;
+        unsigned* lh = reinterpret_cast<unsigned*>(c.dyn);
+        for (int i = threadIdx.x; i < SMILI_NBUCKET; i += blockDim.x) lh[i] = 0;
+        __syncthreads();
+        for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+          const unsigned long long k = c.bkey[i];
+          if (k != ~0ULL) atomicAdd(&lh[bucket_of(k, kmin, shift)], 1u);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < SMILI_NBUCKET; i += blockDim.x)
+          if (lh[i]) atomicAdd(&ghist[i], (int)lh[i]);
+        if (!group_sync(*c.g)) return -2;
+        // exclusive prefix of the bucket counts -> start offsets (in lh)
+        for (int i = threadIdx.x; i < SMILI_NBUCKET; i += blockDim.x) lh[i] = (unsigned)((volatile int*)ghist)[i];
+        __syncthreads();
+        if (threadIdx.x < 32) {
+          // warp 0: sequential chunks of 128 buckets per lane, then a warp scan
+          const int per = SMILI_NBUCKET / 32;
+          unsigned run = 0;
+          for (int q = 0; q < per; ++q) run += lh[threadIdx.x * per + q];
+          unsigned incl = run;
+          for (int s2 = 1; s2 < 32; s2 <<= 1) {
+            const unsigned o = __shfl_up_sync(0xffffffffu, incl, s2);
+            if (threadIdx.x >= s2) incl += o;
+          }
+          unsigned acc2 = incl - run;
+          for (int q = 0; q < per; ++q) {
+            const unsigned v = lh[threadIdx.x * per + q];
+            lh[threadIdx.x * per + q] = acc2;
+            acc2 += v;
+          }
+        }
+        __syncthreads();
+        for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+          const unsigned long long k = c.bkey[i];
+          if (k != ~0ULL) {
+            const int b = bucket_of(k, kmin, shift);
+            const int q = (int)lh[b] + atomicAdd(&ghist[SMILI_NBUCKET + b], 1);
+            sbk[q] = k;
+            sbi[q] = i;
+          }
+        }
+        if (!group_sync(*c.g)) return -2;
+      }
+      if (c.g->rank == 0) cauchy_scan(c, f1, p, nbreak, bnded, sbk, sbi, ghist);
     }
   }
   if (!group_sync(*c.g)) return -2;
@@ -843,8 +961,8 @@ __device__ int lb_formk(LbCtx& c) {
   const int E = 2 * nsym + 2 * m * m;
   const int tpe = SMILI_THREADS / E;  // threads per entry (>= 2 for m <= 6)
   // tile staging: TE elements x (2m values + flag)
-  const int TE = 32;
-  double* tile = reinterpret_cast<double*>(c.dyn);  // [TE][2m+1]
+  const int TE = 256;
+  double* tile = reinterpret_cast<double*>(c.dyn);  // [TE][2m+1] (<= 26 KB)
   const int stride = 2 * m + 1;
   const int my_e = threadIdx.x / tpe, my_sub = threadIdx.x % tpe;
   int kind = -1, ea = 0, eb = 0;
@@ -1237,7 +1355,9 @@ __device__ int lb_iter(LbCtx& c) {
       }
       __syncthreads();
     } else {
+      c.prof->mark(PR_LB_POST);
       const int rc = lb_cauchy(c);
+      c.prof->mark(PR_CAUCHY);
       if (rc == -2) return lb_abort(c);
       if (rc != 0) {
         if (threadIdx.x == 0) reset_memory(S);
@@ -1249,7 +1369,9 @@ __device__ int lb_iter(LbCtx& c) {
     }
     if (S.nfree != 0 && S.col != 0) {
       if (S.wrk) {
+        c.prof->mark(PR_LB_POST);
         const int rc = lb_formk(c);
+        c.prof->mark(PR_FORMK);
         if (rc == -9) return lb_abort(c);
         if (rc != 0) {
           if (threadIdx.x == 0) reset_memory(S);
@@ -1257,7 +1379,9 @@ __device__ int lb_iter(LbCtx& c) {
           continue;
         }
       }
+      c.prof->mark(PR_LB_POST);
       const int rc = lb_cmprlb_subsm(c);
+      c.prof->mark(PR_SUBSM);
       if (rc == -9) return lb_abort(c);
       if (rc != 0) {
         if (threadIdx.x == 0) reset_memory(S);
@@ -1265,7 +1389,9 @@ __device__ int lb_iter(LbCtx& c) {
         continue;
       }
     }
+    c.prof->mark(PR_LB_POST);
     const int r = lb_lnsrch_start(c);
+    c.prof->mark(PR_LNSRCH);
     if (r == LB_RET_ABORT) return lb_abort(c);
     if (r == LB_RET_RESTART) continue;
     return r;

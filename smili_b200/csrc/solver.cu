@@ -25,9 +25,9 @@
 
 #define SMILI_VERSION 1
 #define SMILI_SMEM_CPX 2048   // complex elements per FFT buffer
-#define SMILI_DYN_MIN (40 * 1024)
+#define SMILI_DYN_CPX 6144    // complex elements of dynamic shared memory (96 KB FP64)
 
-enum { MODE_SOLVE = 0, MODE_FG = 1, MODE_T2 = 2, MODE_T1 = 3 };
+enum { MODE_SOLVE = 0, MODE_FG = 1, MODE_T2 = 2, MODE_T1 = 3, MODE_BARRIER = 4 };
 
 struct BatchArgs {
   char* arena;
@@ -40,6 +40,7 @@ struct BatchArgs {
   int* grp_prob;       // [ngroups]
   int* abort_flag;
   ProbResult* results; // [nprob]
+  unsigned long long* prof;  // [PR_NSTAGE] stage times (ns) or null
 };
 
 // ---------------------------------------------------------------------------
@@ -50,6 +51,8 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
                          double* scratch, double& f, double& gd, double& sbg, double* terms,
                          int mode) {
   const ProbDesc& P = *fc.P;
+  Prof& pf = *lc.prof;
+  pf.mark(PR_OTHER);
   double mom[10];
   for (int k = 0; k < 10; ++k) mom[k] = 0.0;
   fg_t2_rows(fc, g, mom);
@@ -67,22 +70,29 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
   } else if (!group_sync(g)) {
     return false;
   }
+  pf.mark(PR_F1);
   fg_t2_cols(fc, g);
   if (!group_sync(g)) return false;
+  pf.mark(PR_F2);
   fg_interp(fc, g);
   if (!group_sync(g)) return false;
+  pf.mark(PR_F3);
   if (mode == MODE_T2) return true;
   double chi[4] = {0, 0, 0, 0};
   if (mode != MODE_T1) {
     fg_chisq(fc, g, chi);
     if (!group_sync(g)) return false;
   }
+  pf.mark(PR_F4);
   fg_spread(fc, g);
   if (!group_sync(g)) return false;
+  pf.mark(PR_F5);
   fg_t1_rows(fc, g);
   if (!group_sync(g)) return false;
+  pf.mark(PR_F6);
   fg_t1_cols(fc, g);
   if (!group_sync(g)) return false;
+  pf.mark(PR_F7);
   if (mode == MODE_T1) return true;
   double acc[14];
   for (int k = 0; k < 14; ++k) acc[k] = 0.0;
@@ -97,6 +107,8 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
   double r[14];
   for (int k = 0; k < 14; ++k) r[k] = red[k];
   __syncthreads();
+  pf.mark(PR_F8);
+  pf.count(PR_COUNT);
   // global-sum regularizers (image.f90:108-135)
   if (P.has_tfd) r[4 + 5] = P.tfd_l * rm.tfd_resid * rm.tfd_resid;
   if (P.has_cen) r[4 + 6] = P.cen_l * rm.cen_cost;
@@ -135,6 +147,10 @@ __global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a)
   __shared__ double scratch[SMILI_WARPS * SMILI_REDK];
   __shared__ int prob_s;
   const int grp = blockIdx.x / a.G, rank = blockIdx.x % a.G;
+  Prof prof;
+  prof.acc = (blockIdx.x == 0 && threadIdx.x == 0) ? a.prof : nullptr;
+  prof.t = 0;
+  prof.start();
   GroupCtx g;
   g.rank = rank;
   g.G = a.G;
@@ -143,6 +159,11 @@ __global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a)
   g.red_out = a.red_out + (size_t)grp * SMILI_REDK;
   g.abort_flag = a.abort_flag;
   g.spin_limit = SMILI_SPIN_LIMIT;
+  if (a.mode == MODE_BARRIER) {  // cost of the group barrier: 1000 waits
+    for (int i = 0; i < 1000; ++i)
+      if (!group_sync(g)) return;
+    return;
+  }
   while (true) {
     if (rank == 0 && threadIdx.x == 0) {
       const int p = atomicAdd(a.queue, 1);
@@ -162,6 +183,7 @@ __global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a)
     fc.sbuf = reinterpret_cast<cpx<R>*>(dyn);
     fc.swork = fc.sbuf + SMILI_SMEM_CPX;
     fc.smem_cpx = SMILI_SMEM_CPX;
+    fc.dyn_cpx = SMILI_DYN_CPX;
     LbCtx lc;
     lc.P = &P;
     lc.base = base;
@@ -190,6 +212,7 @@ __global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a)
     lc.ops = ops;
     lc.scratch = scratch;
     lc.dyn = dyn;
+    lc.prof = &prof;
     const double* x0 = at<double>(base, P.o_x0);
     if (a.mode == MODE_SOLVE) {
       lb_init(lc, x0);
@@ -211,6 +234,7 @@ __global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a)
       __syncthreads();
     }
     bool ok = group_sync(g);
+    prof.mark(PR_INIT);
     double terms_l[SMILI_NTERMS];
     while (ok) {
       double f = 0, gd = 0, sbg = 0;
@@ -226,6 +250,7 @@ __global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a)
       if (S.error) ok = false;
       if (rr != LB_RET_FG) break;
       if (!group_sync(g)) ok = false;
+      prof.mark(PR_LB_POST);
     }
     if (ok && a.mode == MODE_SOLVE) {
       // final summary evaluation at the returned image (fftim2d.f90:356-376)
@@ -503,17 +528,35 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.b2s = (int)mn2;
     d.b2n = (int)(mx2 - mn2 + 1);
   }
-  // sort the uv points by 8x8 tiles of the band for locality; remap indices
+  // sort the uv points by 8x8 bins of the band (spreading subproblems and
+  // locality); remap indices.  Band-relative cells are computed exactly as the
+  // kernels do: imod(ceil(xi - w/2) - start, nf).
+  auto imodh = [](long a, long n) {
+    long r = a % n;
+    return r < 0 ? r + n : r;
+  };
   std::vector<int> perm(nuv);
   std::iota(perm.begin(), perm.end(), 0);
-  {
-    std::vector<long> key(nuv);
-    for (int j = 0; j < nuv; ++j) {
-      const long c1 = (long)std::ceil(xu[j] - half) - d.b1s, c2 = (long)std::ceil(xv[j] - half) - d.b2s;
-      key[j] = ((c2 >> 3) << 32) + (c1 >> 3);
-    }
-    std::stable_sort(perm.begin(), perm.end(), [&](int p, int q) { return key[p] < key[q]; });
+  std::vector<long> bkey(nuv);
+  for (int j = 0; j < nuv; ++j) {
+    const long c1 = imodh((long)std::ceil(xu[j] - half) - d.b1s, d.nf1);
+    const long c2 = imodh((long)std::ceil(xv[j] - half) - d.b2s, d.nf2);
+    bkey[j] = ((c2 >> 3) << 32) + (c1 >> 3);
   }
+  std::stable_sort(perm.begin(), perm.end(), [&](int p, int q) { return bkey[p] < bkey[q]; });
+  // spreading work items: <= 128 consecutive points of one bin
+  std::vector<int> items;
+  for (int j = 0; j < nuv;) {
+    const long k = bkey[perm[j]];
+    int e = j;
+    while (e < nuv && bkey[perm[e]] == k && e - j < 128) ++e;
+    items.push_back(j);
+    items.push_back(e);
+    items.push_back((int)((k >> 32) * 8));
+    items.push_back((int)((k & 0xffffffffL) * 8));
+    j = e;
+  }
+  d.nitems = (int)items.size() / 4;
   std::vector<int> newpos(nuv);
   for (int j = 0; j < nuv; ++j) newpos[perm[j]] = j;
   std::vector<R> su(nuv), sv(nuv);
@@ -638,6 +681,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.o_dsgn = ar.take(dsgn.size());
   d.o_csr_off = ar.take(sizeof(int) * (nuv + 1));
   d.o_csr_ent = ar.take(sizeof(int) * csr_ent.size());
+  d.o_items = ar.take(sizeof(int) * items.size());
   d.o_tmpA = ar.take(C * (size_t)ny * d.b1n);
   d.o_bandA = ar.take(C * (size_t)d.b2n * d.b1n);
   d.o_V = ar.take(C * nuv);
@@ -656,6 +700,9 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.o_iwh = ar.take(N);
     d.o_free = ar.take(N);
     d.o_bkey = ar.take(sizeof(unsigned long long) * N);
+    d.o_sbk = ar.take(sizeof(unsigned long long) * N);
+    d.o_sbi = ar.take(sizeof(int) * N);
+    d.o_hist = ar.take(sizeof(int) * 2 * 4096);
     d.o_lred = ar.take(sizeof(double) * 64);
     d.o_trace = ar.take(sizeof(double) * (niter + 2));
   }
@@ -686,6 +733,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   hp.put(d.o_dsgn, dsgn);
   hp.put(d.o_csr_off, csr_off);
   hp.put(d.o_csr_ent, csr_ent);
+  hp.put(d.o_items, items);
   if (kind == PK_T1) hp.put(d.o_contrib, contrib0);
   // the original -> sorted uv permutation is needed to return visibilities
   hp.blobs.emplace_back(-1, std::vector<char>((const char*)perm.data(), (const char*)perm.data() + sizeof(int) * nuv));
@@ -710,9 +758,11 @@ struct smili_batch {
   double* d_red_out = nullptr;
   int* d_grp_prob = nullptr;
   int* d_abort = nullptr;
+  unsigned long long* d_prof = nullptr;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   size_t dyn_bytes = 0;
+  int profile = 0;
 };
 
 namespace {
@@ -738,6 +788,8 @@ int launch_batch(smili_batch* b, int mode, float* ms) {
   a.grp_prob = b->d_grp_prob;
   a.abort_flag = b->d_abort;
   a.results = b->d_results;
+  a.prof = b->profile ? b->d_prof : nullptr;
+  if (b->profile) CUDA_TRY(cudaMemsetAsync(b->d_prof, 0, sizeof(unsigned long long) * PR_NSTAGE, b->stream));
   void* args[] = {&a};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ms) {
@@ -799,7 +851,9 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
     return fail(SMILI_ERR_NODEV, "cannot select the CUDA device");
   }
   // launch geometry: co-resident CTAs split into groups
-  b->dyn_bytes = std::max((size_t)SMILI_DYN_MIN, 2 * (size_t)SMILI_SMEM_CPX * sizeof(cpx<R>));
+  // FFT/spread staging (SMILI_DYN_CPX complex values) and the Cauchy scan's
+  // batch buffers (about 56 KB) share the dynamic region
+  b->dyn_bytes = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)64 * 1024);
   const void* fn = (const void*)smili_batch_kernel<R>;
   auto cleanup = [&](int rc) {
     smili_batch_destroy(b);
@@ -834,7 +888,8 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
                o_q = take(sizeof(int)), o_bar = take(sizeof(unsigned) * 2 * b->ngroups),
                o_rp = take(sizeof(double) * (size_t)b->ngroups * G * SMILI_REDK),
                o_ro = take(sizeof(double) * (size_t)b->ngroups * SMILI_REDK),
-               o_gp = take(sizeof(int) * b->ngroups), o_ab = take(sizeof(int));
+               o_gp = take(sizeof(int) * b->ngroups), o_ab = take(sizeof(int)),
+               o_pf = take(sizeof(unsigned long long) * PR_NSTAGE);
   if (cudaMalloc(&b->d_aux, aux) != cudaSuccess) return cleanup(fail(SMILI_ERR_CUDA, "cudaMalloc aux failed"));
   b->d_descs = reinterpret_cast<ProbDesc*>(b->d_aux + o_desc);
   b->d_results = reinterpret_cast<ProbResult*>(b->d_aux + o_res);
@@ -844,6 +899,7 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   b->d_red_out = reinterpret_cast<double*>(b->d_aux + o_ro);
   b->d_grp_prob = reinterpret_cast<int*>(b->d_aux + o_gp);
   b->d_abort = reinterpret_cast<int*>(b->d_aux + o_ab);
+  b->d_prof = reinterpret_cast<unsigned long long*>(b->d_aux + o_pf);
   if (opt && opt->stream) {
     b->stream = (cudaStream_t)opt->stream;
   } else {
@@ -904,6 +960,7 @@ int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const 
 
 int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms) {
   if (!b) return fail(SMILI_ERR_ARG, "null batch");
+  if (fg_only == 2) return run(b, MODE_BARRIER, kernel_ms);  // barrier timing (diagnostic)
   return run(b, fg_only ? MODE_FG : MODE_SOLVE, kernel_ms);
 }
 
@@ -922,6 +979,18 @@ int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double
     info->niter = r.iter;
     info->nfg = r.nfg;
     info->error = r.error;
+  }
+  return SMILI_OK;
+}
+
+int smili_batch_profile(smili_batch* b, int enable, double* stage_ns, int len) {
+  if (!b) return fail(SMILI_ERR_ARG, "null batch");
+  b->profile = enable ? 1 : 0;
+  if (stage_ns && len > 0) {
+    unsigned long long h[PR_NSTAGE];
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaMemcpy(h, b->d_prof, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < len; ++i) stage_ns[i] = i < PR_NSTAGE ? (double)h[i] : 0.0;
   }
   return SMILI_OK;
 }

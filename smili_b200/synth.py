@@ -264,22 +264,30 @@ def observe(truth: np.ndarray, img: Image, rng: np.random.Generator, nst: int,
             dec_deg: float, freq_hz: float, hours: float, scan_min: float,
             snr_range=(5.0, 200.0), gain_amp: float = 0.0, gain_phase: bool = False,
             fcv: bool = True, amp: bool = False, cp: bool = True, ca: bool = False,
-            amp_frac_err: float = 0.0, tint_s: float = 10.0):
-    """Simulate a VLBI track of ``truth`` and form the requested tables."""
+            amp_frac_err: float = 0.0, tint_s: float = 10.0, model=None):
+    """Simulate a VLBI track of ``truth`` and form the requested tables.
+
+    ``model(truth, img, u, v)`` returns the model visibilities; the default is
+    the exact DFT ``exact_dft``.  Every baseline is observed in every scan, so
+    row ``scan * Nbl + b`` of the visibility table is baseline ``b``.
+    """
     lam = C_LIGHT / freq_hz
     pos = random_stations(rng, nst)
     nscan = max(1, int(round(hours * 60.0 / scan_min)))
     gst = np.linspace(0.0, hours, nscan, endpoint=False) + rng.uniform(0, 24)
     dec = np.deg2rad(dec_deg)
     bls = list(itertools.combinations(range(nst), 2))
-    rows = []
-    for isc, t in enumerate(gst):
-        for (a, b) in bls:
-            d = pos[b] - pos[a]
-            u, v, w = calc_uvw(t, 0.0, dec, d[0], d[1], d[2])
-            rows.append((isc, a, b, u / lam, v / lam))
-    tab = pd.DataFrame(rows, columns=["scan", "st1", "st2", "u", "v"])
-    V = exact_dft(truth, img, tab["u"].values, tab["v"].values)
+    nbl = len(bls)
+    bidx = {b: i for i, b in enumerate(bls)}
+    ba = np.array([a for a, _ in bls])
+    bb = np.array([b for _, b in bls])
+    dvec = pos[bb] - pos[ba]                                   # (nbl, 3)
+    T = np.repeat(gst, nbl)
+    D = np.tile(dvec, (nscan, 1))
+    u, v, _ = calc_uvw(T, 0.0, dec, D[:, 0], D[:, 1], D[:, 2])
+    tab = pd.DataFrame({"scan": np.repeat(np.arange(nscan), nbl), "st1": np.tile(ba, nscan),
+                        "st2": np.tile(bb, nscan), "u": u / lam, "v": v / lam})
+    V = (model or exact_dft)(truth, img, tab["u"].values, tab["v"].values)
     snr = 10 ** rng.uniform(np.log10(snr_range[0]), np.log10(snr_range[1]), V.size)
     sigma = np.abs(V) / snr
     if gain_amp > 0 or gain_phase:
@@ -301,49 +309,49 @@ def observe(truth: np.ndarray, img: Image, rng: np.random.Generator, nst: int,
         if amp_frac_err > 0:
             at["sigma"] = np.sqrt(at["sigma"] ** 2 + (amp_frac_err * at["amp"]) ** 2)
         out["amptable"] = at
-    key = {(r.scan, r.st1, r.st2): i for i, r in enumerate(tab.itertuples(index=False))}
     U, Vv = tab["u"].values, tab["v"].values
     A, P, S = tab["amp"].values, np.deg2rad(tab["phase"].values), tab["sigma"].values
+    base = (np.arange(nscan) * nbl)[:, None]
     if cp:
-        brow = []
-        for isc in range(nscan):
-            for i in range(1, nst):
-                for j in range(i + 1, nst):
-                    k1, k2, k3 = key[(isc, 0, i)], key[(isc, i, j)], key[(isc, 0, j)]
-                    r1, r2, r3 = S[k1] / A[k1], S[k2] / A[k2], S[k3] / A[k3]
-                    bamp = A[k1] * A[k2] * A[k3]
-                    ph = P[k1] + P[k2] - P[k3]
-                    brow.append((U[k1], Vv[k1], U[k2], Vv[k2], -U[k3], -Vv[k3], bamp,
-                                 np.rad2deg(np.angle(np.exp(1j * ph))),
-                                 bamp * math.sqrt(r1 * r1 + r2 * r2 + r3 * r3)))
-        out["bstable"] = pd.DataFrame(brow, columns=["u12", "v12", "u23", "v23", "u31", "v31",
-                                                     "amp", "phase", "sigma"])
+        tri = [(0, i, j) for i in range(1, nst) for j in range(i + 1, nst)]
+        k1 = (base + np.array([bidx[(0, i)] for _, i, _ in tri])[None, :]).ravel()
+        k2 = (base + np.array([bidx[(i, j)] for _, i, j in tri])[None, :]).ravel()
+        k3 = (base + np.array([bidx[(0, j)] for _, _, j in tri])[None, :]).ravel()
+        bamp = A[k1] * A[k2] * A[k3]
+        ph = P[k1] + P[k2] - P[k3]
+        out["bstable"] = pd.DataFrame({
+            "u12": U[k1], "v12": Vv[k1], "u23": U[k2], "v23": Vv[k2], "u31": -U[k3], "v31": -Vv[k3],
+            "amp": bamp, "phase": np.rad2deg(np.angle(np.exp(1j * ph))),
+            "sigma": bamp * np.sqrt((S[k1] / A[k1]) ** 2 + (S[k2] / A[k2]) ** 2 + (S[k3] / A[k3]) ** 2)})
     if ca:
         quads = _independent_quads(nst)
-        crow = []
-        for isc in range(nscan):
+        ks = []
+        for pair_sel in range(4):
+            col = []
             for (a, b, c, d) in quads:
-                ks = [key[(isc,) + tuple(sorted(p))] for p in ((a, b), (c, d), (a, c), (b, d))]
-                rho2 = [max(1.0, (A[k] / S[k]) ** 2 - 1) for k in ks]
-                lamp = math.log(A[ks[0]]) + math.log(A[ks[1]]) - math.log(A[ks[2]]) - math.log(A[ks[3]])
-                lsig = math.sqrt(sum(1.0 / r for r in rho2))
-                crow.append((U[ks[0]], Vv[ks[0]], U[ks[1]], Vv[ks[1]], U[ks[2]], Vv[ks[2]],
-                             U[ks[3]], Vv[ks[3]], math.exp(lamp), lamp, lsig))
-        out["catable"] = pd.DataFrame(crow, columns=["u1", "v1", "u2", "v2", "u3", "v3", "u4", "v4",
-                                                     "amp", "logamp", "logsigma"])
+                pr = ((a, b), (c, d), (a, c), (b, d))[pair_sel]
+                col.append(bidx[tuple(sorted(pr))])
+            ks.append((base + np.array(col)[None, :]).ravel())
+        rho2 = [np.maximum(1.0, (A[k] / S[k]) ** 2 - 1) for k in ks]
+        lamp = np.log(A[ks[0]]) + np.log(A[ks[1]]) - np.log(A[ks[2]]) - np.log(A[ks[3]])
+        lsig = np.sqrt(sum(1.0 / r for r in rho2))
+        out["catable"] = pd.DataFrame({
+            "u1": U[ks[0]], "v1": Vv[ks[0]], "u2": U[ks[1]], "v2": Vv[ks[1]],
+            "u3": U[ks[2]], "v3": Vv[ks[2]], "u4": U[ks[3]], "v4": Vv[ks[3]],
+            "amp": np.exp(lamp), "logamp": lamp, "logsigma": lsig})
     return out
 
 
 # ----------------------------------------------------------------------------
 # the named workloads
 # ----------------------------------------------------------------------------
-def small_crescent(seed: int = 0, nx: int = 64, niter: int = 1000) -> Observation:
+def small_crescent(seed: int = 0, nx: int = 64, niter: int = 1000, model=None) -> Observation:
     """64x64, 2 uas pixels, blurred crescent, 8 stations, fcv + cp, l1 = tsv = 1."""
     rng = np.random.default_rng(seed)
     img = Image(nx, nx, 2.0)
     truth = crescent_image(img)
     t = observe(truth, img, rng, nst=8, dec_deg=12.0, freq_hz=230e9, hours=12.0,
-                scan_min=10.0, fcv=True, cp=True)
+                scan_min=10.0, fcv=True, cp=True, model=model)
     init = img.copy()
     init.data[0, 0] = gaussian_image(img, 20.0, 0.6)
     return Observation(init, truth, t["vistable"], None, t["bstable"], None,
@@ -351,7 +359,7 @@ def small_crescent(seed: int = 0, nx: int = 64, niter: int = 1000) -> Observatio
 
 
 def precision_path(seed: int = 1, nx: int = 256, nst: int = 10, hours: float = 12.0,
-                   scan_s: float = 20.0, niter: int = 1000) -> Observation:
+                   scan_s: float = 20.0, niter: int = 1000, model=None) -> Observation:
     """256x256, 1 uas, 50 Gaussians + GP, 10 stations, ~1e5 vis with gain errors;
     log closure amplitudes + closure phases + 5% amplitudes; l1/TV/MEM = 1/1/0.1."""
     rng = np.random.default_rng(seed)
@@ -359,7 +367,7 @@ def precision_path(seed: int = 1, nx: int = 256, nst: int = 10, hours: float = 1
     truth = multigauss_gp_image(img, rng)
     t = observe(truth, img, rng, nst=nst, dec_deg=12.0, freq_hz=230e9, hours=hours,
                 scan_min=scan_s / 60.0, gain_amp=0.1, gain_phase=True, fcv=False,
-                amp=True, cp=True, ca=True, amp_frac_err=0.05)
+                amp=True, cp=True, ca=True, amp_frac_err=0.05, model=model)
     init = img.copy()
     tf = float(t["amptable"]["amp"].max())
     init.data[0, 0] = gaussian_image(img, 60.0, tf)
@@ -367,7 +375,7 @@ def precision_path(seed: int = 1, nx: int = 256, nst: int = 10, hours: float = 1
                        {"l1_lambda": 1.0, "tv_lambda": 1.0, "kl_lambda": 0.1}, niter, tf)
 
 
-def survey_problem(index: int, seed: int = 3, niter: int = 1000) -> Observation:
+def survey_problem(index: int, seed: int = 3, niter: int = 1000, model=None) -> Observation:
     """One problem of the hyper-parameter survey: N in {64..256}, Nvis log-uniform
     2e3-5e4, 6-12 stations, (l1, tsv, mem) on an 8x8x8 log grid 1e-2..1e2."""
     rng = np.random.default_rng([seed, index])
@@ -387,7 +395,7 @@ def survey_problem(index: int, seed: int = 3, niter: int = 1000) -> Observation:
     else:
         truth = gaussian_image(img, 30.0, 0.8, 5.0, -3.0)
     t = observe(truth, img, rng, nst=nst, dec_deg=float(rng.uniform(-30, 60)), freq_hz=230e9,
-                hours=hours, scan_min=hours * 60.0 / nscan, fcv=True, cp=True)
+                hours=hours, scan_min=hours * 60.0 / nscan, fcv=True, cp=True, model=model)
     grid = np.logspace(-2, 2, 8)
     li = np.unravel_index(index % 512, (8, 8, 8))
     init = img.copy()
@@ -396,3 +404,20 @@ def survey_problem(index: int, seed: int = 3, niter: int = 1000) -> Observation:
     return Observation(init, truth, t["vistable"], None, t["bstable"], None,
                        {"l1_lambda": float(grid[li[0]]), "tsv_lambda": float(grid[li[1]]),
                         "kl_lambda": float(grid[li[2]])}, niter, tf)
+
+
+def nufft_model(truth: np.ndarray, img: Image, u: np.ndarray, v: np.ndarray,
+                eps: float = 1e-12) -> np.ndarray:
+    """Model visibilities through the library's own type-2 NUFFT (GPU).
+
+    Same convention as ``exact_dft``: the NUFFT phase origin is pixel
+    nx/2+1, so the result is rotated to the reference pixel nxref.
+    """
+    from .fortlib import fftlib
+    h = img.header
+    up = u * (2 * np.pi * np.deg2rad(h["dx"]))
+    vp = v * (2 * np.pi * np.deg2rad(h["dy"]))
+    vr, vi = fftlib.nufft_fwd_real(up, vp, np.asarray(truth).T, nufft_eps=eps)
+    dix = h["nx"] // 2 + 1 - h["nxref"]
+    diy = h["ny"] // 2 + 1 - h["nyref"]
+    return (vr + 1j * vi) * np.exp(1j * (up * dix + vp * diy))
