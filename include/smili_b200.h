@@ -32,6 +32,7 @@ extern "C" {
 #define SMILI_TASK_ABNORMAL 4  /* ABNORMAL_TERMINATION_IN_LNSRCH */
 #define SMILI_TASK_STOP 5      /* STOP: TOTAL ITERATION NUMBER EXCEEDS LIMIT */
 #define SMILI_TASK_ERROR 6
+#define SMILI_TASK_TARGET 8    /* reached the target set by smili_batch_set_targets */
 
 /* The arguments of fortlib.fftim2d.imaging / calc_cost
  * (src/fortlib/fftim2d.f90:11-34, smili/imaging/lbfgs.py:492-564). */
@@ -104,6 +105,10 @@ int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const 
 int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms);
 int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double* grad,
                       smili_solve_info* info);
+/* Per-problem objective targets (no reference counterpart): a solve stops
+ * with SMILI_TASK_TARGET at the first completed iteration whose cost is
+ * <= ftarget[p]; niter stays the iteration cap.  NULL clears the targets. */
+int smili_batch_set_targets(smili_batch* b, const double* ftarget);
 /* Cost recorded at each completed iteration of problem p (NaN where absent). */
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len);
 void smili_batch_destroy(smili_batch* b);

@@ -63,11 +63,12 @@ class SolveInfo(C.Structure):
 
 TERM_NAMES = ["chisq", "chisqfcv", "chisqamp", "chisqcp", "chisqca", "reg", "l1_cost", "tv_cost",
               "tsv_cost", "kl_cost", "gs_cost", "tfd_cost", "cen_cost", "sm_cost", "cost"]
-TASK_CONV, TASK_ABNORMAL, TASK_STOP, TASK_ERROR = 3, 4, 5, 6
+TASK_CONV, TASK_ABNORMAL, TASK_STOP, TASK_ERROR, TASK_TARGET = 3, 4, 5, 6, 8
 
 EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "smili_batch_run",
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
-           "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile"]
+           "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile",
+           "smili_batch_set_targets"]
 STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
           "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
           "c_gather", "c_sort", "c_scan", "c_rounds"]
@@ -93,6 +94,7 @@ def lib():
         L.smili_batch_destroy.argtypes = [vp]
         L.smili_batch_destroy.restype = None
         L.smili_batch_profile.argtypes = [vp, C.c_int, dp, C.c_int]
+        L.smili_batch_set_targets.argtypes = [vp, dp]
         L.smili_nufft_fwd_real.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp, vp, dp, dp]
         L.smili_nufft_adj_real1d.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, vp, dp]
         _lib = L
@@ -193,6 +195,14 @@ class Batch:
         check(lib().smili_batch_fetch(self.h, p, dptr(x), dptr(terms), dptr(g), C.byref(info)))
         return x, dict(zip(TERM_NAMES, terms)), g, {"task": info.task, "niter": info.niter,
                                                      "nfg": info.nfg, "error": info.error}
+
+    def set_targets(self, ftarget):
+        """Stop problem p once its cost <= ftarget[p] (None clears)."""
+        if ftarget is None:
+            check(lib().smili_batch_set_targets(self.h, None))
+        else:
+            t = np.ascontiguousarray(np.broadcast_to(np.asarray(ftarget, dtype=np.float64), (self.n,)))
+            check(lib().smili_batch_set_targets(self.h, dptr(t)))
 
     def profile(self, enable=True):
         check(lib().smili_batch_profile(self.h, int(bool(enable)), None, 0))

@@ -102,32 +102,49 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   return v;
 }
 
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned atom_acqrel_add(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// Wait until the generation counter moves past gen.  Polls without sleeping
+// for a short while (barriers normally complete within microseconds), then
+// backs off; gives up after spin_limit polls or when another CTA aborted.
+__device__ __forceinline__ bool wait_generation(GroupCtx& g, unsigned gen) {
+  long long spins = 0;
+  while (ld_acquire(&g.bar[1]) == gen) {
+    if (++spins > g.spin_limit || *((volatile int*)g.abort_flag)) {
+      atomicExch(g.abort_flag, 1);
+      return false;
+    }
+    if (spins > 4096) __nanosleep(64);
+  }
+  return true;
+}
+
 // Returns false when the wait timed out (abort flag set): callers stop work.
+// Arrival is an acquire-release atomic on the group's counter (it orders this
+// CTA's earlier writes before the arrival and the last arriver's reads after
+// it); the last arriver resets the counter and releases the generation.
 __device__ bool group_sync(GroupCtx& g) {
   __syncthreads();
   if (g.G == 1) return true;
   __shared__ int ok_s;
   if (threadIdx.x == 0) {
     int ok = 1;
+    __threadfence();  // writes of the whole block (ordered by bar.sync) before the arrival
     const unsigned gen = ld_acquire(&g.bar[1]);
-    __threadfence();
-    const unsigned arrived = atomicAdd(&g.bar[0], 1u);
+    const unsigned arrived = atom_acqrel_add(&g.bar[0], 1u);
     if (arrived == (unsigned)(g.G - 1)) {
       g.bar[0] = 0;
-      __threadfence();
-      atomicAdd(&g.bar[1], 1u);
+      red_release_add(&g.bar[1], 1u);
     } else {
-      long long spins = 0;
-      while (ld_acquire(&g.bar[1]) == gen) {
-        if (++spins > g.spin_limit || *((volatile int*)g.abort_flag)) {
-          atomicExch(g.abort_flag, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
-      }
+      ok = wait_generation(g, gen) ? 1 : 0;
     }
-    __threadfence();
     ok_s = ok;
   }
   __syncthreads();
@@ -146,48 +163,33 @@ __device__ bool group_reduce(GroupCtx& g, double* vals, const unsigned char* ops
     return true;
   }
   __shared__ int last_s, ok_s;
-  for (int k = threadIdx.x; k < K; k += blockDim.x) {
-    g.red_part[(size_t)g.rank * SMILI_REDK + k] = vals[k];
-    __threadfence();
-  }
+  for (int k = threadIdx.x; k < K; k += blockDim.x) g.red_part[(size_t)g.rank * SMILI_REDK + k] = vals[k];
   __syncthreads();
   if (threadIdx.x == 0) {
     ok_s = 1;
     last_s = 0;
-    __threadfence();
+    __threadfence();  // the block's partials (written by other threads) before the arrival
     const unsigned gen = ld_acquire(&g.bar[1]);
-    const unsigned arrived = atomicAdd(&g.bar[0], 1u);
+    const unsigned arrived = atom_acqrel_add(&g.bar[0], 1u);
     if (arrived == (unsigned)(g.G - 1)) {
       last_s = 1;
     } else {
-      long long spins = 0;
-      while (ld_acquire(&g.bar[1]) == gen) {
-        if (++spins > g.spin_limit || *((volatile int*)g.abort_flag)) {
-          atomicExch(g.abort_flag, 1);
-          ok_s = 0;
-          break;
-        }
-        __nanosleep(32);
-      }
-      __threadfence();
+      ok_s = wait_generation(g, gen) ? 1 : 0;
     }
   }
   __syncthreads();
   if (last_s) {
-    __threadfence();
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
       const volatile double* rp = g.red_part;
       double a = rp[k];
       for (int r = 1; r < g.G; ++r) a = red_op(a, rp[(size_t)r * SMILI_REDK + k], ops[k]);
       g.red_out[k] = a;
-      __threadfence();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      __threadfence();
+      __threadfence();  // the reduced values before the release
       g.bar[0] = 0;
-      __threadfence();
-      atomicAdd(&g.bar[1], 1u);
+      red_release_add(&g.bar[1], 1u);
     }
   }
   __syncthreads();

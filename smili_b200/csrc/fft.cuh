@@ -112,10 +112,12 @@ __device__ cpx<R>* smem_fft(cpx<R>* buf, cpx<R>* work, const FftPlan& pl, int S,
     const int Rr = pl.rad[p];
     const int nr = n / Rr;
     const int tstep = n / (Ns * Rr);
+    // (s, j) = divmod(idx, nr) advanced incrementally as idx steps by
+    // blockDim.x; one division per step (for k = j mod Ns) instead of three
+    int s = threadIdx.x / nr, j = threadIdx.x - (threadIdx.x / nr) * nr;
+    const int ds = blockDim.x / nr, dj = blockDim.x - ds * nr;
+    int jq = j / Ns, k = j - jq * Ns;
     for (int idx = threadIdx.x; idx < S * nr; idx += blockDim.x) {
-      const int s = idx / nr;
-      const int j = idx - s * nr;
-      const int k = j % Ns;
       const cpx<R>* in = src + (size_t)s * n;
       cpx<R> v[8];
       for (int r = 0; r < Rr; ++r) {
@@ -130,8 +132,17 @@ __device__ cpx<R>* smem_fft(cpx<R>* buf, cpx<R>* work, const FftPlan& pl, int S,
         case 3: dft3(v); break;
         default: dft5(v); break;
       }
-      cpx<R>* out = dst + (size_t)s * n + (j / Ns) * Ns * Rr + k;
+      cpx<R>* out = dst + (size_t)s * n + jq * Ns * Rr + k;
       for (int r = 0; r < Rr; ++r) out[r * Ns] = v[r];
+      // advance to idx + blockDim.x
+      s += ds;
+      j += dj;
+      if (j >= nr) {
+        j -= nr;
+        ++s;
+      }
+      jq = j / Ns;  // Ns is a power of the radices; one division per step
+      k = j - jq * Ns;
     }
     __syncthreads();
     cpx<R>* t = src;

@@ -25,9 +25,12 @@ __device__ __forceinline__ R es_kernel(R z, R beta) {
 }
 
 __device__ __forceinline__ int imod(int a, int n) {
+  if ((unsigned)a < (unsigned)n) return a;  // the common case
   int r = a % n;
   return r < 0 ? r + n : r;
 }
+// a in (-n, 2n): one conditional add or subtract
+__device__ __forceinline__ int wrapn(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
 
 __device__ __forceinline__ double smabs(double x) { return sqrt(x * x + 1e-10); }
 
@@ -99,7 +102,7 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
       const int s = i / nx, ix = i - s * nx, iy = row0 + s;
       const int pv = inv[iy * nx + ix];
       const double val = pv >= 0 ? x[pv] : 0.0;
-      c.sbuf[s * n1 + imod(ix - nx / 2, n1)] = cmk<R>((R)(val * dc1[ix] * dc2[iy]), (R)0);
+      c.sbuf[s * n1 + wrapn(ix - nx / 2, n1)] = cmk<R>((R)(val * dc1[ix] * dc2[iy]), (R)0);
       if (need_mom && pv >= 0) {
         const double fx = ix + 1, fy = iy + 1;  // 1-based pixel numbers as the reference
         mom[0] += val;
@@ -121,7 +124,7 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
     const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, rows, tw1);
     for (int i = threadIdx.x; i < rows * P.b1n; i += blockDim.x) {
       const int s = i / P.b1n, b = i - s * P.b1n;
-      tmpA[(size_t)(row0 + s) * P.b1n + b] = out[s * n1 + imod(P.b1s + b, n1)];
+      tmpA[(size_t)(row0 + s) * P.b1n + b] = out[s * n1 + wrapn(P.b1s + b, n1)];
     }
     __syncthreads();
   }
@@ -145,13 +148,13 @@ __device__ void fg_t2_cols(FgCtx<R>& c, const GroupCtx& g) {
     __syncthreads();
     for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
       const int iy = i / cols, s = i - iy * cols;
-      c.sbuf[s * n2 + imod(iy - ny / 2, n2)] = tmpA[(size_t)iy * b1n + b0 + s];
+      c.sbuf[s * n2 + wrapn(iy - ny / 2, n2)] = tmpA[(size_t)iy * b1n + b0 + s];
     }
     __syncthreads();
     const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, cols, tw2);
     for (int i = threadIdx.x; i < cols * P.b2n; i += blockDim.x) {
       const int b2 = i / cols, s = i - b2 * cols;
-      bandA[(size_t)b2 * b1n + b0 + s] = out[s * n2 + imod(P.b2s + b2, n2)];
+      bandA[(size_t)b2 * b1n + b0 + s] = out[s * n2 + wrapn(P.b2s + b2, n2)];
     }
     __syncthreads();
   }
@@ -455,13 +458,13 @@ __device__ void fg_t1_rows(FgCtx<R>& c, const GroupCtx& g) {
     __syncthreads();
     for (int i = threadIdx.x; i < rows * b1n; i += blockDim.x) {
       const int s = i / b1n, b = i - s * b1n;
-      c.sbuf[s * n1 + imod(P.b1s + b, n1)] = bandC[(size_t)(r0 + s) * b1n + b];
+      c.sbuf[s * n1 + wrapn(P.b1s + b, n1)] = bandC[(size_t)(r0 + s) * b1n + b];
     }
     __syncthreads();
     const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, rows, tw1);
     for (int i = threadIdx.x; i < rows * nx; i += blockDim.x) {
       const int s = i / nx, ix = i - s * nx;
-      tmpC[(size_t)(r0 + s) * nx + ix] = out[s * n1 + imod(ix - nx / 2, n1)];
+      tmpC[(size_t)(r0 + s) * nx + ix] = out[s * n1 + wrapn(ix - nx / 2, n1)];
     }
     __syncthreads();
   }
@@ -487,13 +490,13 @@ __device__ void fg_t1_cols(FgCtx<R>& c, const GroupCtx& g) {
     __syncthreads();
     for (int i = threadIdx.x; i < cols * P.b2n; i += blockDim.x) {
       const int b2 = i / cols, s = i - b2 * cols;
-      c.sbuf[s * n2 + imod(P.b2s + b2, n2)] = tmpC[(size_t)b2 * nx + x0 + s];
+      c.sbuf[s * n2 + wrapn(P.b2s + b2, n2)] = tmpC[(size_t)b2 * nx + x0 + s];
     }
     __syncthreads();
     const cpx<R>* out = smem_fft(c.sbuf, c.swork, pl, cols, tw2);
     for (int i = threadIdx.x; i < cols * ny; i += blockDim.x) {
       const int iy = i / cols, s = i - iy * cols, ix = x0 + s;
-      gchi[(size_t)iy * nx + ix] = (double)out[s * n2 + imod(iy - ny / 2, n2)].x * dc1[ix] * dc2[iy];
+      gchi[(size_t)iy * nx + ix] = (double)out[s * n2 + wrapn(iy - ny / 2, n2)].x * dc1[ix] * dc2[iy];
     }
     __syncthreads();
   }

@@ -23,7 +23,8 @@ enum {
   LB_TASK_ABNORMAL = 4,   // line search failed with an empty memory
   LB_TASK_STOP = 5,       // iteration limit reached (iter > niter)
   LB_TASK_ERROR = 6,      // invalid input or a device-side wait timed out
-  LB_TASK_FG_ONLY = 7     // single evaluation, no optimisation
+  LB_TASK_FG_ONLY = 7,    // single evaluation, no optimisation
+  LB_TASK_TARGET = 8      // reached the requested objective value
 };
 
 struct ProbDesc {
@@ -46,6 +47,7 @@ struct ProbDesc {
   double sm_l, sm_maj, sm_min, sm_phi;
   double nxref, nyref;
   double factr, pgtol;
+  double ftarget;          // stop once f <= ftarget at a completed iteration (-inf: off)
   // byte offsets in the arena (0 = absent)
   int64_t o_x0, o_xidx, o_yidx, o_inv;
   int64_t o_l1w, o_tvw, o_tsvw, o_klw, o_gsw;

@@ -397,7 +397,7 @@ __device__ void block_scan_incl(double* vals, int V, double* wtot /* shared [WAR
 // (key - kmin) >> shift, with the shift chosen so that the keys span at most
 // SMILI_NBUCKET buckets.  sbk/sbi receive the breakpoints grouped by bucket in
 // increasing bucket order (unordered inside a bucket); hist the bucket counts.
-#define SMILI_NBUCKET 4096
+#define SMILI_NBUCKET 2048
 
 __device__ __forceinline__ int bucket_of(unsigned long long k, unsigned long long kmin, int shift) {
   const unsigned long long q = (k - kmin) >> shift;
@@ -494,7 +494,7 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
   const double theta = S.theta;
   // shared layout inside dyn
   u128* cand = reinterpret_cast<u128*>(c.dyn);                        // SMILI_KC
-  unsigned* hist = reinterpret_cast<unsigned*>(cand + SMILI_KC);      // 4096 (bucket counts)
+  unsigned* hist = reinterpret_cast<unsigned*>(cand + SMILI_KC);      // NBUCKET (bucket counts)
   unsigned* hist2 = hist + SMILI_NBUCKET;                             // 4096 (fallback)
   double* wtot = reinterpret_cast<double*>(hist2 + 4096);             // WARPS*32
   double* dtm_s = wtot + SMILI_WARPS * 32;                            // THREADS
@@ -1455,7 +1455,10 @@ __device__ int lb_after_fg(LbCtx& c, double f, double gd_fg, double sbg) {
     S.iter++;
     S.sbgnrm = sbg;
     if (c.g->rank == 0 && S.iter - 1 < P.niter + 2) c.trace[S.iter - 1] = S.f;
-    if (S.iter > P.niter) {
+    if (S.f <= P.ftarget) {
+      S.task = LB_TASK_TARGET;  // requested objective reached (no reference counterpart)
+      S.done = 1;
+    } else if (S.iter > P.niter) {
       S.task = LB_TASK_STOP;  // fftim2d.f90:324-325
       S.done = 1;
     } else if (S.sbgnrm <= P.pgtol) {

@@ -139,7 +139,7 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
 }
 
 template <typename R>
-__global__ void __launch_bounds__(SMILI_THREADS) smili_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(SMILI_THREADS, sizeof(R) == 4 ? 3 : 2) smili_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) char dyn[];
   __shared__ LbState S;
   __shared__ double red[SMILI_REDK];
@@ -437,6 +437,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.nonneg = nonneg ? 1 : 0;
   d.factr = factr;
   d.pgtol = pgtol;
+  d.ftarget = -INFINITY;
   d.prec64 = sizeof(R) == 8;
   d.nxref = a.nxref;
   d.nyref = a.nyref;
@@ -852,8 +853,9 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   }
   // launch geometry: co-resident CTAs split into groups
   // FFT/spread staging (SMILI_DYN_CPX complex values) and the Cauchy scan's
-  // batch buffers (about 56 KB) share the dynamic region
-  b->dyn_bytes = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)64 * 1024);
+  // batch buffers (about 47 KB) share the dynamic region: 96 KB in FP64 (two
+  // CTAs per SM), 48 KB in FP32 (three CTAs per SM)
+  b->dyn_bytes = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
   const void* fn = (const void*)smili_batch_kernel<R>;
   auto cleanup = [&](int rc) {
     smili_batch_destroy(b);
@@ -992,6 +994,16 @@ int smili_batch_profile(smili_batch* b, int enable, double* stage_ns, int len) {
     CUDA_TRY(cudaMemcpy(h, b->d_prof, sizeof(h), cudaMemcpyDeviceToHost));
     for (int i = 0; i < len; ++i) stage_ns[i] = i < PR_NSTAGE ? (double)h[i] : 0.0;
   }
+  return SMILI_OK;
+}
+
+int smili_batch_set_targets(smili_batch* b, const double* ftarget) {
+  if (!b) return fail(SMILI_ERR_ARG, "null batch");
+  for (int p = 0; p < b->nprob; ++p) b->descs[p].ftarget = ftarget ? ftarget[p] : -INFINITY;
+  CUDA_TRY(cudaSetDevice(b->device));
+  CUDA_TRY(cudaMemcpyAsync(b->d_descs, b->descs.data(), sizeof(ProbDesc) * b->nprob, cudaMemcpyHostToDevice,
+                           b->stream));
+  CUDA_TRY(cudaStreamSynchronize(b->stream));
   return SMILI_OK;
 }
 

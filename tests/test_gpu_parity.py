@@ -168,3 +168,31 @@ def test_invalid_inputs_raise(crescent32, lib):
     with pytest.raises(lib.SmiliError) as e:
         lib.Batch([bad], niter=5)
     assert e.value.code == -2
+
+
+def test_target_stop(crescent32, lib):
+    """A solve with an objective target stops at the first completed
+    iteration whose cost is at or below it; without a target it runs on."""
+    kw = make_kw(crescent32, niter=40)
+    opts = lib.make_options(64, 1e-9)
+    b = lib.Batch([kw, kw], niter=40, options=opts)
+    b.run()
+    tr = b.trace(0, 42)
+    assert b.fetch(0)[3]["task"] == lib.TASK_STOP
+    k = 15
+    assert tr[k] < tr[k - 1]
+    target = 0.5 * (tr[k - 1] + tr[k])  # robust to run-to-run rounding
+    first = int(np.argmax(tr <= target))
+    assert first == k
+    b.set_targets([target, -np.inf])
+    b.run()
+    _, t0, _, i0 = b.fetch(0)
+    _, t1, _, i1 = b.fetch(1)
+    assert i0["task"] == lib.TASK_TARGET
+    assert i0["niter"] == first + 1
+    assert t0["cost"] <= target
+    assert i1["task"] == lib.TASK_STOP and i1["niter"] == 41
+    b.set_targets(None)
+    b.run()
+    assert b.fetch(0)[3]["task"] == lib.TASK_STOP
+    b.close()
