@@ -1142,3 +1142,145 @@ int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const doub
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free calc_cost (no reference counterpart)
+//
+// The same evaluation as smili_calc_cost, with the problem arena and the
+// launch's bookkeeping placed in one file-scope device array instead of
+// cudaMalloc'd buffers.  It calls no CUDA allocator and no allocating
+// library: its device scratch is g_noalloc_scratch, whose address is taken
+// once per device with cudaGetSymbolAddress.  Problems whose arena does not
+// fit are rejected with SMILI_ERR_ARG.  The one scratch array is shared by
+// all calls on a device, so calls that overlap in time (other threads or
+// streams) race; the first call on a device performs the set-up and should
+// come before any stream capture.
+// ===========================================================================
+#include <mutex>
+
+namespace {
+
+constexpr size_t kNoAllocBytes = (size_t)SMILI_NOALLOC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDev = 64;
+std::mutex g_noalloc_mu;
+char* g_noalloc_ptr[kNoAllocMaxDev] = {};
+
+// device address of the scratch array on `device` (which must be current)
+int noalloc_scratch(int device, char** out) {
+  if (device < 0 || device >= kNoAllocMaxDev) return fail(SMILI_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (!p || (reinterpret_cast<uintptr_t>(p) & 255u))
+      return fail(SMILI_ERR_CUDA, "scratch symbol address is null or not 256-byte aligned");
+    const size_t dyn64 = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<double>), (size_t)48 * 1024);
+    const size_t dyn32 = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<float>), (size_t)48 * 1024);
+    CUDA_TRY(cudaFuncSetAttribute((const void*)smili_batch_kernel<double>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn64));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)smili_batch_kernel<float>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn32));
+    g_noalloc_ptr[device] = static_cast<char*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return SMILI_OK;
+}
+
+size_t round256(size_t n) { return (n + 255) / 256 * 256; }
+
+template <typename R>
+int calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_options* opt, double* terms,
+                      double* grad) {
+  const double eps = (opt && opt->nufft_eps > 0) ? opt->nufft_eps : 1e-6;
+  const int device = opt ? opt->device : 0;
+  if (!(eps < 1.0)) return fail(SMILI_ERR_ARG, "nufft_eps must be in (0, 1)");
+  Arena ar;
+  HostProb hp;
+  int rc = pack_problem<R>(*a, PK_FG, 0, 0, 5, 1e1, 0.0, eps, ar, hp, x, nullptr, nullptr);
+  if (rc != SMILI_OK) return rc;
+  const size_t arena_al = round256(std::max<size_t>(ar.bytes, 256));
+  if (arena_al > kNoAllocBytes)
+    return fail(SMILI_ERR_ARG, "smili_calc_cost_noalloc: the problem needs " + std::to_string(arena_al) +
+                                   " bytes of device scratch, more than the " + std::to_string(kNoAllocBytes) +
+                                   " of the static scratch; use smili_calc_cost");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) return fail(SMILI_ERR_NODEV, "no CUDA device");
+  if (cudaSetDevice(device) != cudaSuccess) return fail(SMILI_ERR_NODEV, "cannot select the CUDA device");
+  char* scratch = nullptr;
+  rc = noalloc_scratch(device, &scratch);
+  if (rc != SMILI_OK) return rc;
+  // launch geometry for one problem (as in create_batch)
+  smili_batch b;  // host bookkeeping only: every device pointer points into the scratch
+  b.nprob = 1;
+  b.prec64 = sizeof(R) == 8;
+  b.device = device;
+  b.kind = PK_FG;
+  b.descs.push_back(hp.d);
+  b.dyn_bytes = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
+  const void* fn = (const void*)smili_batch_kernel<R>;
+  int occ = 0, nsm = 0, coop = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, SMILI_THREADS, b.dyn_bytes));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  if (!coop || occ < 1) return fail(SMILI_ERR_CUDA, "cooperative launch unavailable");
+  const int maxres = occ * nsm;
+  int G = opt && opt->ctas_per_problem > 0 ? opt->ctas_per_problem : 0;
+  if (G <= 0) G = std::max(1, std::min(maxres, (hp.d.npix + 1023) / 1024));
+  G = std::min(G, maxres);
+  b.G = G;
+  b.ngroups = 1;
+  // bookkeeping after the arena, laid out as in create_batch
+  size_t off = arena_al;
+  auto take = [&](size_t n) {
+    const size_t o = off;
+    off += round256(n);
+    return o;
+  };
+  const size_t o_desc = take(sizeof(ProbDesc)), o_res = take(sizeof(ProbResult)), o_q = take(sizeof(int)),
+               o_bar = take(sizeof(unsigned) * 2), o_rp = take(sizeof(double) * (size_t)G * SMILI_REDK),
+               o_ro = take(sizeof(double) * SMILI_REDK), o_gp = take(sizeof(int)), o_ab = take(sizeof(int)),
+               o_pf = take(sizeof(unsigned long long) * PR_NSTAGE);
+  if (off > kNoAllocBytes)
+    return fail(SMILI_ERR_ARG, "smili_calc_cost_noalloc: the problem needs " + std::to_string(off) +
+                                   " bytes of device scratch, more than the " + std::to_string(kNoAllocBytes) +
+                                   " of the static scratch; use smili_calc_cost");
+  b.d_arena = scratch;
+  b.arena_bytes = ar.bytes;
+  b.d_aux = scratch + arena_al;
+  b.d_descs = reinterpret_cast<ProbDesc*>(scratch + o_desc);
+  b.d_results = reinterpret_cast<ProbResult*>(scratch + o_res);
+  b.d_queue = reinterpret_cast<int*>(scratch + o_q);
+  b.d_bars = reinterpret_cast<unsigned*>(scratch + o_bar);
+  b.d_red_part = reinterpret_cast<double*>(scratch + o_rp);
+  b.d_red_out = reinterpret_cast<double*>(scratch + o_ro);
+  b.d_grp_prob = reinterpret_cast<int*>(scratch + o_gp);
+  b.d_abort = reinterpret_cast<int*>(scratch + o_ab);
+  b.d_prof = reinterpret_cast<unsigned long long*>(scratch + o_pf);
+  b.stream = (opt && opt->stream) ? (cudaStream_t)opt->stream : cudaStreamPerThread;
+  b.own_stream = false;
+  // what must start at zero: the arena (as the allocating path clears it);
+  // the queue, barrier counters and abort flag are cleared by launch_batch
+  CUDA_TRY(cudaMemsetAsync(b.d_arena, 0, arena_al, b.stream));
+  for (auto& bl : hp.blobs) {
+    if (bl.first < 0 || bl.second.empty()) continue;  // host-side permutation; not needed for calc_cost
+    CUDA_TRY(cudaMemcpyAsync(b.d_arena + bl.first, bl.second.data(), bl.second.size(), cudaMemcpyHostToDevice,
+                             b.stream));
+  }
+  CUDA_TRY(cudaMemcpyAsync(b.d_descs, b.descs.data(), sizeof(ProbDesc), cudaMemcpyHostToDevice, b.stream));
+  rc = launch_batch<R>(&b, MODE_FG, nullptr);
+  if (rc != SMILI_OK) return rc;
+  return smili_batch_fetch(&b, 0, nullptr, terms, grad, nullptr);
+}
+
+}  // namespace
+
+extern "C" int smili_calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_options* opt,
+                                       double* terms, double* grad) {
+  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+  const int prec = opt && opt->precision ? opt->precision : 64;
+  if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
+  return prec == 64 ? calc_cost_noalloc<double>(a, x, opt, terms, grad)
+                    : calc_cost_noalloc<float>(a, x, opt, terms, grad);
+}

@@ -42,3 +42,18 @@ def calc_cost(x, precision=64, nufft_eps=0.0, device=0, **kw):
     _lib.check(_lib.lib().smili_calc_cost(C.addressof(prob.c), _lib.dptr(x), C.byref(opt),
                                           _lib.dptr(terms), _lib.dptr(grad)))
     return dict(zip(_lib.TERM_NAMES, terms)), grad
+
+
+def calc_cost_noalloc(x, precision=64, nufft_eps=0.0, device=0, **kw):
+    """calc_cost through the allocation-free entry point: the same result as
+    ``calc_cost`` for problems whose device arena fits the library's static
+    scratch (others raise SmiliError with code -1).  Calls on one device
+    must not overlap."""
+    prob = _lib.Problem(kw)
+    opt = _lib.make_options(precision, nufft_eps, 0, device)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    terms = np.zeros(15)
+    grad = np.zeros(prob.npix)
+    _lib.check(_lib.lib().smili_calc_cost_noalloc(C.addressof(prob.c), _lib.dptr(x), C.byref(opt),
+                                                  _lib.dptr(terms), _lib.dptr(grad)))
+    return dict(zip(_lib.TERM_NAMES, terms)), grad
