@@ -406,6 +406,39 @@ def survey_problem(index: int, seed: int = 3, niter: int = 1000, model=None) -> 
                         "kl_lambda": float(grid[li[2]])}, niter, tf)
 
 
+def warmstart_problem(seed: int, nx: int = 128, niter: int = 1000, model=None) -> Observation:
+    """One problem of the learned-warm-start set: 1 uas pixels; truth a
+    crescent, ring, multi-Gaussian or GP-texture source (by seed mod 4) with
+    seeded shape and total flux; 6-12 seeded stations, 12 h track with 10 min
+    scans, SNR log-uniform 5-200; complex visibilities + closure phases;
+    l1 = tsv = 1; a 20 uas Gaussian prior with the zero-spacing flux."""
+    rng = np.random.default_rng([seed, 44])
+    img = Image(nx, nx, 1.0)
+    flux = float(10 ** rng.uniform(np.log10(0.3), np.log10(1.5)))
+    kind = seed % 4
+    if kind in (0, 1):
+        r_out = float(rng.uniform(15.0, 30.0))
+        truth = crescent_image(img, r_out_uas=r_out, r_in_uas=r_out * float(rng.uniform(0.5, 0.8)),
+                               shift_uas=0.0 if kind == 1 else float(rng.uniform(2.0, 0.3 * r_out)),
+                               flux=flux, blur_fwhm_uas=float(rng.uniform(3.0, 8.0)),
+                               angle=float(rng.uniform(0, 2 * np.pi)))
+    elif kind == 2:
+        truth = multigauss_gp_image(img, rng, ngauss=int(rng.integers(3, 13)), flux=flux,
+                                    extent_uas=25.0, gp_frac=0.05)
+    else:
+        truth = multigauss_gp_image(img, rng, ngauss=int(rng.integers(2, 6)), flux=flux,
+                                    extent_uas=20.0, gp_corr_uas=float(rng.uniform(5.0, 12.0)),
+                                    gp_frac=float(rng.uniform(0.6, 0.9)))
+    nst = int(rng.integers(6, 13))
+    t = observe(truth, img, rng, nst=nst, dec_deg=float(rng.uniform(-30, 60)), freq_hz=230e9,
+                hours=12.0, scan_min=10.0, fcv=True, cp=True, model=model)
+    tf = float(t["vistable"]["amp"].max())
+    init = img.copy()
+    init.data[0, 0] = gaussian_image(img, 20.0, tf)
+    return Observation(init, truth, t["vistable"], None, t["bstable"], None,
+                       {"l1_lambda": 1.0, "tsv_lambda": 1.0}, niter, tf)
+
+
 def nufft_model(truth: np.ndarray, img: Image, u: np.ndarray, v: np.ndarray,
                 eps: float = 1e-12) -> np.ndarray:
     """Model visibilities through the library's own type-2 NUFFT (GPU).

@@ -104,16 +104,29 @@ class UNet:
                            L.b.detach().cpu().numpy().copy())
         return out
 
-    def save(self, path):
-        p = self.params()
-        np.savez(path, channels=np.array(self.c), **{f"{k}_w": v[0] for k, v in p.items()},
-                 **{f"{k}_b": v[1] for k, v in p.items()})
+    def save(self, path, bf16=True):
+        """Weights (bf16 bit patterns as uint16 when ``bf16``, else float32)
+        and float32 biases."""
+        p = self.params_bf16() if bf16 else self.params()
+
+        def enc(w):
+            w = np.ascontiguousarray(w, np.float32)
+            return (w.view(np.uint32) >> 16).astype(np.uint16) if bf16 else w
+
+        np.savez(path, channels=np.array(self.c), bf16=np.array(bool(bf16)),
+                 **{f"{k}_w": enc(v[0]) for k, v in p.items()}, **{f"{k}_b": v[1] for k, v in p.items()})
 
     @classmethod
     def load(cls, path, device="cuda"):
         z = np.load(path)
         net = cls(tuple(int(c) for c in z["channels"]), device=device)
-        net.set_params({L.name: (z[f"{L.name}_w"], z[f"{L.name}_b"]) for L in net.layers})
+
+        def dec(w):
+            if w.dtype == np.uint16:
+                return (w.astype(np.uint32) << 16).view(np.float32)
+            return w
+
+        net.set_params({L.name: (dec(z[f"{L.name}_w"]), z[f"{L.name}_b"]) for L in net.layers})
         return net
 
     def _flip_all(self):
