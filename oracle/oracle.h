@@ -75,6 +75,49 @@ int orc_imaging(const orc_args* a, int niter, int nonneg, int nprint, int m, dou
                 double pgtol, double eps, double* iout, double* terms, double* trace,
                 int* nfg, int* niter_done, int* task);
 
+/* Arguments of fortlib.fftim3d.imaging / calc_cost (fftim3d.f90:11-44,
+ * 473-498): a movie of nz frames of npix pixels (frame-major), u/v the
+ * concatenation of the frames' uv lists with nuvs[nz] points per frame. */
+typedef struct {
+  int npix, nx, ny, nz;
+  const double* iin;
+  const int* xidx;
+  const int* yidx;
+  double nxref, nyref;
+  int nuv;
+  const double* u;
+  const double* v;
+  const int* nuvs;
+  double l1_l;  const double* l1_wgt;
+  double tv_l;  const double* tv_wgt;
+  double tsv_l; const double* tsv_wgt;
+  double kl_l;  const double* kl_wgt;
+  double gs_l;  const double* gs_wgt;
+  double tfd_l, tfd_tgtfd;
+  const double* lc_l;
+  const double* lc_tgtfd;
+  int lc_nidx;
+  double cen_l, cen_alpha;
+  double sm_l, sm_maj, sm_min, sm_phi;
+  double rt_l; const double* rt_wgt;
+  double ri_l; const double* ri_wgt;
+  double rs_l, rf_l;
+  int isfcv, nfcv; const int* uvidxfcv; const double* vfcvr; const double* vfcvi; const double* varfcv; double wfcv;
+  int isamp, namp; const int* uvidxamp; const double* vamp; const double* varamp; double wamp;
+  int iscp, ncp;   const int* uvidxcp;  const double* cp;   const double* varcp;  double wcp;
+  int isca, nca;   const int* uvidxca;  const double* ca;   const double* varca;  double wca;
+  double inormfactr;
+} orc_args3d;
+
+/* terms[20] = chisq, chisqfcv, chisqamp, chisqcp, chisqca, reg, l1, sm, tv,
+ * tsv, kl, gs, tfd, lc, cen, rt, ri, rs, rf, cost (fftim3d.imaging order). */
+int orc_calc_cost3d(const orc_args3d* a, const double* vfcv_shifted_re, const double* vfcv_shifted_im,
+                    double wfcv_n, double wamp_n, double wcp_n, double wca_n,
+                    const double* x, double eps, double* terms, double* grad);
+int orc_imaging3d(const orc_args3d* a, int niter, int nonneg, int nprint, int m, double factr,
+                  double pgtol, double eps, double* iout, double* terms, double* trace,
+                  int* nfg, int* niter_done, int* task);
+
 /* Reverse-communication L-BFGS-B restatement (src/lbfgsb/lbfgsb.f).
  * nbd: 0 none, 1 lower, 2 both, 3 upper.  Returns a task code
  * (see ORC_TASK_*). */

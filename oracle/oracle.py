@@ -41,6 +41,10 @@ def lib():
                                        C.c_double, dp, C.c_double, dp, dp]
         _lib.orc_imaging.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                      C.c_double, C.c_double, dp, dp, dp, ip, ip, ip]
+        _lib.orc_calc_cost3d.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, dp, C.c_double, dp, dp]
+        _lib.orc_imaging3d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                       C.c_double, C.c_double, dp, dp, dp, ip, ip, ip]
         _lib.orc_lbfgsb_new.restype = C.c_void_p
         _lib.orc_lbfgsb_new.argtypes = [C.c_int, C.c_int, dp, dp, ip, C.c_double, C.c_double]
         _lib.orc_lbfgsb_step.argtypes = [C.c_void_p, dp, C.c_double, dp]
@@ -205,6 +209,101 @@ def imaging(kw: dict, eps=1e-6, trace_len=None):
                       _d(trace), C.byref(nfg), C.byref(nit), C.byref(task))
     return iout, dict(zip(TERM_NAMES, terms)), {"nfg": nfg.value, "niter": nit.value,
                                                   "task": task.value, "trace": trace}
+
+
+class _Args3d(C.Structure):
+    _fields_ = [
+        ("npix", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("iin", C.c_void_p), ("xidx", C.c_void_p), ("yidx", C.c_void_p),
+        ("nxref", C.c_double), ("nyref", C.c_double),
+        ("nuv", C.c_int), ("u", C.c_void_p), ("v", C.c_void_p), ("nuvs", C.c_void_p),
+        ("l1_l", C.c_double), ("l1_wgt", C.c_void_p), ("tv_l", C.c_double), ("tv_wgt", C.c_void_p),
+        ("tsv_l", C.c_double), ("tsv_wgt", C.c_void_p), ("kl_l", C.c_double), ("kl_wgt", C.c_void_p),
+        ("gs_l", C.c_double), ("gs_wgt", C.c_void_p),
+        ("tfd_l", C.c_double), ("tfd_tgtfd", C.c_double),
+        ("lc_l", C.c_void_p), ("lc_tgtfd", C.c_void_p), ("lc_nidx", C.c_int),
+        ("cen_l", C.c_double), ("cen_alpha", C.c_double),
+        ("sm_l", C.c_double), ("sm_maj", C.c_double), ("sm_min", C.c_double), ("sm_phi", C.c_double),
+        ("rt_l", C.c_double), ("rt_wgt", C.c_void_p), ("ri_l", C.c_double), ("ri_wgt", C.c_void_p),
+        ("rs_l", C.c_double), ("rf_l", C.c_double),
+        ("isfcv", C.c_int), ("nfcv", C.c_int), ("uvidxfcv", C.c_void_p), ("vfcvr", C.c_void_p),
+        ("vfcvi", C.c_void_p), ("varfcv", C.c_void_p), ("wfcv", C.c_double),
+        ("isamp", C.c_int), ("namp", C.c_int), ("uvidxamp", C.c_void_p), ("vamp", C.c_void_p),
+        ("varamp", C.c_void_p), ("wamp", C.c_double),
+        ("iscp", C.c_int), ("ncp", C.c_int), ("uvidxcp", C.c_void_p), ("cp", C.c_void_p),
+        ("varcp", C.c_void_p), ("wcp", C.c_double),
+        ("isca", C.c_int), ("nca", C.c_int), ("uvidxca", C.c_void_p), ("ca", C.c_void_p),
+        ("varca", C.c_void_p), ("wca", C.c_double),
+        ("inormfactr", C.c_double),
+    ]
+
+
+TERM_NAMES_3D = ["chisq", "chisqfcv", "chisqamp", "chisqcp", "chisqca", "reg", "l1_cost", "sm_cost",
+                 "tv_cost", "tsv_cost", "kl_cost", "gs_cost", "tfd_cost", "lc_cost", "cen_cost",
+                 "rt_cost", "ri_cost", "rs_cost", "rf_cost", "cost"]
+
+
+class Args3d(Args):
+    """fortlib.fftim3d.imaging kwargs (fftim3d.f90:11-44) as a C struct."""
+
+    def __init__(self, kw: dict):
+        f64 = lambda k: np.ascontiguousarray(np.asarray(kw[k], dtype=np.float64).reshape(-1))
+        i32 = lambda k: np.ascontiguousarray(np.asarray(kw[k], dtype=np.int32).reshape(-1))
+        self.keep = {}
+        a = _Args3d()
+        for k in ["iin", "u", "v", "l1_wgt", "tv_wgt", "tsv_wgt", "kl_wgt", "gs_wgt", "lc_l", "lc_tgtfd",
+                  "rt_wgt", "ri_wgt", "vfcvr", "vfcvi", "varfcv", "vamp", "varamp", "cp", "varcp", "ca",
+                  "varca"]:
+            self.keep[k] = f64(k)
+        for k in ["xidx", "yidx", "uvidxfcv", "uvidxamp", "nuvs"]:
+            self.keep[k] = i32(k)
+        self.keep["uvidxcp"] = np.ascontiguousarray(np.asarray(kw["uvidxcp"], dtype=np.int32).T).reshape(-1)
+        self.keep["uvidxca"] = np.ascontiguousarray(np.asarray(kw["uvidxca"], dtype=np.int32).T).reshape(-1)
+        for k, arr in self.keep.items():
+            setattr(a, k, arr.ctypes.data)
+        a.npix = int(kw["npix"])
+        a.nx, a.ny, a.nz = int(kw["nx"]), int(kw["ny"]), int(kw["nz"])
+        a.nxref, a.nyref = float(kw["nxref"]), float(kw["nyref"])
+        a.nuv = self.keep["u"].size
+        for k in ["l1_l", "tv_l", "tsv_l", "kl_l", "gs_l", "tfd_l", "tfd_tgtfd", "cen_l", "cen_alpha",
+                  "sm_l", "sm_maj", "sm_min", "sm_phi", "rt_l", "ri_l", "rs_l", "rf_l", "wfcv", "wamp", "wcp",
+                  "wca", "inormfactr"]:
+            setattr(a, k, float(kw[k]))
+        a.lc_nidx = int(kw["lc_nidx"])
+        a.isfcv, a.isamp, a.iscp, a.isca = (int(bool(kw[k])) for k in ["isfcv", "isamp", "iscp", "isca"])
+        a.nfcv = self.keep["uvidxfcv"].size
+        a.namp = self.keep["uvidxamp"].size
+        a.ncp = self.keep["uvidxcp"].size // 3
+        a.nca = self.keep["uvidxca"].size // 4
+        self.c = a
+        self.kw = kw
+
+
+def calc_cost3d(kw: dict, x, eps=1e-6):
+    """calc_cost of fftim3d at movie vector x (npix * nz): (terms dict, grad)."""
+    a = kw if isinstance(kw, Args3d) else Args3d(kw)
+    vr, vi = a.shifted_fcv()
+    w = a.weights()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    terms = np.zeros(20)
+    grad = np.zeros(a.c.npix * a.c.nz)
+    lib().orc_calc_cost3d(C.byref(a.c), _d(vr), _d(vi), *w, _d(x), float(eps), _d(terms), _d(grad))
+    return dict(zip(TERM_NAMES_3D, terms)), grad
+
+
+def imaging3d(kw: dict, eps=1e-6, trace_len=None):
+    """fftim3d.imaging on the CPU.  Returns (Iout, terms dict, info dict)."""
+    a = Args3d(kw)
+    niter = int(kw["niter"])
+    iout = np.zeros(a.c.npix * a.c.nz)
+    terms = np.zeros(20)
+    trace = np.full(trace_len or niter + 2, np.nan)
+    nfg, nit, task = C.c_int(0), C.c_int(0), C.c_int(0)
+    lib().orc_imaging3d(C.byref(a.c), niter, int(bool(kw["nonneg"])), int(kw["nprint"]), int(kw["m"]),
+                        float(kw["factr"]), float(kw["pgtol"]), float(eps), _d(iout), _d(terms), _d(trace),
+                        C.byref(nfg), C.byref(nit), C.byref(task))
+    return iout, dict(zip(TERM_NAMES_3D, terms)), {"nfg": nfg.value, "niter": nit.value,
+                                                     "task": task.value, "trace": trace}
 
 
 TASK_FG, TASK_NEW_X, TASK_CONV, TASK_ABNORMAL, TASK_ERROR, TASK_STOP = 1, 2, 3, 4, 5, 6

@@ -11,6 +11,7 @@
 // under OpenMP array reductions are summed here in a fixed order so the oracle
 // is deterministic.
 #include "oracle.h"
+#include "oracle_internal.h"
 
 #include <algorithm>
 #include <cmath>
@@ -18,15 +19,11 @@
 #include <cstring>
 #include <vector>
 
-typedef std::complex<double> cplx;
-
-namespace {
+namespace orc {
 
 const double kZeroEps = 1e-10;  // image.f90:7
 
-inline double smabs(double x) { return std::sqrt(x * x + kZeroEps); }
 inline double smabs_diff(double x) { return x / smabs(x); }
-inline int isign(int v) { return v >= 0 ? 1 : -1; }
 
 // --------------------------- chi-square terms ------------------------------
 // fftlib.f90:384-439
@@ -198,10 +195,8 @@ void xy_cen(const double* I, const int* x, const int* y, int n, double& xc, doub
   yc /= tot;
 }
 
-}  // namespace
-
 // calc_cost_reg (image.f90:12-200).  reg[9] = cost, l1, tv, tsv, kl, gs, tfd, cen, sm
-static void calc_cost_reg(const orc_args* a, const double* I1d, double* reg, double* grad) {
+void calc_cost_reg(const orc_args* a, const double* I1d, double* reg, double* grad) {
   const int N = a->npix;
   double l1c = 0, tvc = 0, tsvc = 0, gsc = 0, klc = 0, tfdc = 0, cenc = 0, smc = 0;
   std::fill(grad, grad + N, 0.0);
@@ -306,6 +301,10 @@ static void calc_cost_reg(const orc_args* a, const double* I1d, double* reg, dou
   reg[8] = smc;
   reg[0] = l1c + tvc + tsvc + klc + gsc + tfdc + cenc + smc;
 }
+
+}  // namespace orc
+
+using namespace orc;
 
 // calc_cost (fftim2d.f90:387-607) = calc_chisq (fftlib.f90:250-382) + calc_cost_reg
 extern "C" int orc_calc_cost(const orc_args* a, const double* vre_s, const double* vim_s,

@@ -264,17 +264,21 @@ def observe(truth: np.ndarray, img: Image, rng: np.random.Generator, nst: int,
             dec_deg: float, freq_hz: float, hours: float, scan_min: float,
             snr_range=(5.0, 200.0), gain_amp: float = 0.0, gain_phase: bool = False,
             fcv: bool = True, amp: bool = False, cp: bool = True, ca: bool = False,
-            amp_frac_err: float = 0.0, tint_s: float = 10.0, model=None):
+            amp_frac_err: float = 0.0, tint_s: float = 10.0, model=None, stations=None,
+            gst_start=None):
     """Simulate a VLBI track of ``truth`` and form the requested tables.
 
     ``model(truth, img, u, v)`` returns the model visibilities; the default is
-    the exact DFT ``exact_dft``.  Every baseline is observed in every scan, so
+    the exact DFT ``exact_dft``.  ``stations`` (ECEF positions) and
+    ``gst_start`` (hours) fix the array and the track start instead of drawing
+    them, so that consecutive frames of a movie share one array.  Every baseline is observed in every scan, so
     row ``scan * Nbl + b`` of the visibility table is baseline ``b``.
     """
     lam = C_LIGHT / freq_hz
-    pos = random_stations(rng, nst)
+    pos = random_stations(rng, nst) if stations is None else np.asarray(stations)
     nscan = max(1, int(round(hours * 60.0 / scan_min)))
-    gst = np.linspace(0.0, hours, nscan, endpoint=False) + rng.uniform(0, 24)
+    gst = np.linspace(0.0, hours, nscan, endpoint=False) + (rng.uniform(0, 24) if gst_start is None
+                                                             else gst_start)
     dec = np.deg2rad(dec_deg)
     bls = list(itertools.combinations(range(nst), 2))
     nbl = len(bls)
@@ -437,6 +441,60 @@ def warmstart_problem(seed: int, nx: int = 128, niter: int = 1000, model=None) -
     init.data[0, 0] = gaussian_image(img, 20.0, tf)
     return Observation(init, truth, t["vistable"], None, t["bstable"], None,
                        {"l1_lambda": 1.0, "tsv_lambda": 1.0}, niter, tf)
+
+
+@dataclasses.dataclass
+class MovieObservation:
+    """A synthetic movie data set: per-frame initial images and truths, and
+    tables with a ``frmidx`` column, ordered by frame."""
+    frames: list                  # initial Image of every frame
+    truths: list                  # (ny, nx) truth of every frame
+    vistable: Optional[pd.DataFrame]
+    bstable: Optional[pd.DataFrame]
+    reg: dict
+    niter: int
+    totalflux: float
+
+
+def dynamic_problem(seed: int = 0, nframes: int = 64, nx: int = 128, nst: int = 16, hours: float = 24.0,
+                    vis_per_frame: int = 6000, niter: int = 1000, model=None) -> MovieObservation:
+    """Dynamic imaging: ``nframes`` frames of nx x nx (1 uas pixels) over a
+    ``hours`` track, ~``vis_per_frame`` visibilities per frame from ``nst``
+    seeded stations; the truth is a crescent rotating by 90 deg over the
+    sequence; complex visibilities + closure phases per frame; l1 = tsv = 1
+    per frame and the inter-frame squared difference Rt = 1."""
+    rng = np.random.default_rng([seed, 55])
+    img = Image(nx, nx, 1.0)
+    pos = random_stations(rng, nst)
+    dec = float(rng.uniform(-30, 60))
+    gst0 = float(rng.uniform(0, 24))
+    window = hours / nframes
+    nbl = nst * (nst - 1) // 2
+    nscan = max(1, int(round(vis_per_frame / nbl)))
+    angle0 = float(rng.uniform(0, 2 * np.pi))
+    truths, vis, bs = [], [], []
+    for z in range(nframes):
+        ang = angle0 + 0.5 * np.pi * z / max(1, nframes - 1)
+        truth = crescent_image(img, r_out_uas=22.0, r_in_uas=15.0, shift_uas=5.0, flux=0.6,
+                               blur_fwhm_uas=5.0, angle=ang)
+        t = observe(truth, img, rng, nst=nst, dec_deg=dec, freq_hz=230e9, hours=window,
+                    scan_min=window * 60.0 / nscan, fcv=True, cp=True, model=model, stations=pos,
+                    gst_start=gst0 + z * window)
+        t["vistable"]["frmidx"] = z
+        t["bstable"]["frmidx"] = z
+        truths.append(truth)
+        vis.append(t["vistable"])
+        bs.append(t["bstable"])
+    vistable = pd.concat(vis, ignore_index=True)
+    bstable = pd.concat(bs, ignore_index=True)
+    tf = 0.6
+    frames = []
+    for z in range(nframes):
+        f = img.copy()
+        f.data[0, 0] = gaussian_image(img, 20.0, tf)
+        frames.append(f)
+    return MovieObservation(frames, truths, vistable, bstable,
+                            {"l1_lambda": 1.0, "tsv_lambda": 1.0, "rt_lambda": 1.0}, niter, tf)
 
 
 def nufft_model(truth: np.ndarray, img: Image, u: np.ndarray, v: np.ndarray,

@@ -93,3 +93,48 @@ def get_uvlist(fcvtable=None, amptable=None, bstable=None, catable=None):
     else:
         uvidxca = np.zeros([4, 1], dtype=np.int32, order="F")
     return (u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca)
+
+
+def get_uvlist_loop(Nt, fcvconcat=None, ampconcat=None, bsconcat=None, caconcat=None):
+    """Per-frame uv lists of a movie, concatenated (tools.py:255-335).
+
+    Every table carries a ``frmidx`` column; frame i's rows go through
+    ``get_uvlist`` on their own and the frame's indices are offset by the
+    number of uv points of the frames before it.  Returns ``(u, v, uvidxfcv,
+    uvidxamp, uvidxcp, uvidxca, Nuvs)``; the data rows must be ordered by
+    frame, as the index arrays are concatenated frame by frame.
+    """
+    if fcvconcat is None and ampconcat is None and bsconcat is None and caconcat is None:
+        print("Error: No data are input.")
+        return -1
+    u, v = [], []
+    idx = {"fcv": [], "amp": [], "cp": [], "ca": []}
+    Nuvs = []
+    offset = 0
+    for i in range(Nt):
+        parts = {}
+        for key, tab in (("fcv", fcvconcat), ("amp", ampconcat), ("cp", bsconcat), ("ca", caconcat)):
+            if tab is None:
+                continue
+            rows = np.where(np.asarray(tab["frmidx"]) == i)[0]
+            if rows.size:
+                parts[key] = tab.iloc[rows]
+        if not parts:
+            Nuvs.append(0)
+            continue
+        u0, v0, ifcv, iamp, icp, ica = get_uvlist(fcvtable=parts.get("fcv"), amptable=parts.get("amp"),
+                                                  bstable=parts.get("cp"), catable=parts.get("ca"))
+        u.append(u0)
+        v.append(v0)
+        Nuvs.append(len(u0))
+        for key, arr in (("fcv", ifcv), ("amp", iamp), ("cp", icp), ("ca", ica)):
+            if key in parts:
+                idx[key].append(np.sign(arr) * (np.abs(arr) + offset))
+        offset += len(u0)
+    u = np.concatenate(u)
+    v = np.concatenate(v)
+    uvidxfcv = np.concatenate(idx["fcv"]) if fcvconcat is not None else np.zeros(1, dtype=np.int32)
+    uvidxamp = np.concatenate(idx["amp"]) if ampconcat is not None else np.zeros(1, dtype=np.int32)
+    uvidxcp = np.hstack(idx["cp"]) if bsconcat is not None else np.zeros([3, 1], dtype=np.int32, order="F")
+    uvidxca = np.hstack(idx["ca"]) if caconcat is not None else np.zeros([4, 1], dtype=np.int32, order="F")
+    return u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca, np.asarray(Nuvs)

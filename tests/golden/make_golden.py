@@ -72,6 +72,22 @@ def main(ref_root: str):
                              bstable=t.get("bs"), catable=t.get("ca"))
         _save(name, t, out)
         print(name, "nuv", len(out[0]))
+    # 4) movies: get_uvlist_loop (tools.py:255-335) over frame-tagged tables,
+    #    frame 2 without data
+    m = synth.dynamic_problem(seed=3, nframes=5, nx=32, nst=6, vis_per_frame=60)
+    keep_v = m.vistable[m.vistable.frmidx != 2].reset_index(drop=True)
+    keep_b = m.bstable[m.bstable.frmidx != 2].reset_index(drop=True)
+    out = ref.get_uvlist_loop(Nt=5, fcvconcat=keep_v, bsconcat=keep_b)
+    arrays = {}
+    for key, tab in (("fcv", keep_v), ("bs", keep_b)):
+        for col in tab.columns:
+            if col.startswith("u") or col.startswith("v") or col == "frmidx":
+                arrays[f"{key}__{col}"] = np.asarray(tab[col], dtype=np.float64)
+    u, v, ifcv, iamp, icp, ica, nuvs = out
+    np.savez_compressed(os.path.join(HERE, "uvlistloop_fcv_cp.npz"), u=u, v=v, uvidxfcv=np.asarray(ifcv),
+                        uvidxamp=np.asarray(iamp), uvidxcp=np.asarray(icp), uvidxca=np.asarray(ica),
+                        nuvs=np.asarray(nuvs), **arrays)
+    print("loop nuv", len(u), "nuvs", list(nuvs))
 
 
 if __name__ == "__main__":

@@ -34,3 +34,18 @@ def test_uvlist_no_data_returns_minus_one():
 
 def test_golden_fixture_count():
     assert len(GOLD) >= 6
+
+
+def test_uvlist_loop_matches_reference():
+    """get_uvlist_loop (movies) against the reference's output on a 5-frame
+    movie whose frame 2 has no data (Nuvs[2] == 0)."""
+    from smili_b200.uvdata.tools import get_uvlist_loop
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "uvlistloop_fcv_cp.npz"))
+    tabs = {}
+    for k in z.files:
+        if "__" in k:
+            t, c = k.split("__")
+            tabs.setdefault(t, {})[c] = z[k]
+    out = get_uvlist_loop(5, fcvconcat=pd.DataFrame(tabs["fcv"]), bsconcat=pd.DataFrame(tabs["bs"]))
+    for got, name in zip(out, ["u", "v", "uvidxfcv", "uvidxamp", "uvidxcp", "uvidxca", "nuvs"]):
+        np.testing.assert_array_equal(np.asarray(got), z[name], err_msg=name)
