@@ -120,6 +120,59 @@ void smili_batch_destroy(smili_batch* b);
  * other, evaluation count. */
 int smili_batch_profile(smili_batch* b, int enable, double* stage_ns, int len);
 
+/* The arguments of fortlib.fftim3d.imaging / calc_cost (dynamic imaging,
+ * src/fortlib/fftim3d.f90:11-44, smili/imaging/lbfgs3d.py:732-784): a movie
+ * of nz frames of npix pixels each (iin frame-major), u/v the frames' uv
+ * lists concatenated with nuvs[nz] points per frame (get_uvlist_loop), data
+ * indices into that list.  Every closure quantity must lie within one frame.
+ * Weights of the static regularizers have npix entries; lc_l / lc_tgtfd
+ * have nz; rs / rf are accepted but, as in the reference, not evaluated. */
+typedef struct {
+  int npix, nx, ny, nz;
+  const double* iin;
+  const int* xidx;
+  const int* yidx;
+  double nxref, nyref;
+  int nuv;
+  const double* u;
+  const double* v;
+  const int* nuvs;
+  double l1_l;  const double* l1_wgt;  int l1_nwgt;
+  double sm_l, sm_maj, sm_min, sm_phi;
+  double tv_l;  const double* tv_wgt;  int tv_nwgt;
+  double tsv_l; const double* tsv_wgt; int tsv_nwgt;
+  double kl_l;  const double* kl_wgt;  int kl_nwgt;
+  double gs_l;  const double* gs_wgt;  int gs_nwgt;
+  double tfd_l, tfd_tgtfd;
+  const double* lc_l;
+  const double* lc_tgtfd;
+  int lc_nidx;
+  double cen_l, cen_alpha;
+  double rt_l; const double* rt_wgt; int rt_nwgt;
+  double ri_l; const double* ri_wgt; int ri_nwgt;
+  double rs_l; const double* rs_wgt; int rs_nwgt;
+  double rf_l; const double* rf_wgt; int rf_nwgt;
+  int isfcv, nfcv; const int* uvidxfcv; const double* vfcvr; const double* vfcvi; const double* varfcv; double wfcv;
+  int isamp, namp; const int* uvidxamp; const double* vamp; const double* varamp; double wamp;
+  int iscp, ncp;   const int* uvidxcp;  const double* cp;   const double* varcp;  double wcp;
+  int isca, nca;   const int* uvidxca;  const double* ca;   const double* varca;  double wca;
+  double inormfactr;
+} smili_imaging3d_args;
+
+/* terms3d[20] = chisq, chisqfcv, chisqamp, chisqcp, chisqca, reg, l1_cost,
+ * sm_cost, tv_cost, tsv_cost, kl_cost, gs_cost, tfd_cost, lc_cost,
+ * cen_cost, rt_cost, ri_cost, rs_cost, rf_cost, cost (fftim3d.f90:41-44). */
+
+/* fortlib.fftim3d.imaging (fftim3d.f90:11-467): one L-BFGS-B solve over all
+ * npix * nz values; Iout is thresholded at 1e-10 like fftim3d.f90:466. */
+int smili_fftim3d_imaging(const smili_imaging3d_args* a, int niter, int nonneg, int nprint, int m,
+                          double factr, double pgtol, const smili_options* opt, double* iout,
+                          double* terms3d, smili_solve_info* info);
+
+/* calc_cost of fftim3d (fftim3d.f90:473-614) at the movie vector x. */
+int smili_calc_cost3d(const smili_imaging3d_args* a, const double* x, const smili_options* opt,
+                      double* terms3d, double* grad);
+
 /* NUFFTs of the imaging path with the reference's conventions (sign "+",
  * modes -N/2..(N-1)/2 at pixels 1..N): fortlib.fftlib.nufft_fwd_real
  * (type 2, fftlib.f90:86-100) and nufft_adj_real1d (type 1, real part,

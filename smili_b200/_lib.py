@@ -57,18 +57,54 @@ class Options(C.Structure):
                 ("device", C.c_int), ("stream", C.c_void_p)]
 
 
+class ImagingArgs3D(C.Structure):
+    """``smili_imaging3d_args``: the arguments of fortlib.fftim3d.imaging."""
+    _fields_ = [
+        ("npix", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("iin", C.c_void_p), ("xidx", C.c_void_p), ("yidx", C.c_void_p),
+        ("nxref", C.c_double), ("nyref", C.c_double),
+        ("nuv", C.c_int), ("u", C.c_void_p), ("v", C.c_void_p), ("nuvs", C.c_void_p),
+        ("l1_l", C.c_double), ("l1_wgt", C.c_void_p), ("l1_nwgt", C.c_int),
+        ("sm_l", C.c_double), ("sm_maj", C.c_double), ("sm_min", C.c_double), ("sm_phi", C.c_double),
+        ("tv_l", C.c_double), ("tv_wgt", C.c_void_p), ("tv_nwgt", C.c_int),
+        ("tsv_l", C.c_double), ("tsv_wgt", C.c_void_p), ("tsv_nwgt", C.c_int),
+        ("kl_l", C.c_double), ("kl_wgt", C.c_void_p), ("kl_nwgt", C.c_int),
+        ("gs_l", C.c_double), ("gs_wgt", C.c_void_p), ("gs_nwgt", C.c_int),
+        ("tfd_l", C.c_double), ("tfd_tgtfd", C.c_double),
+        ("lc_l", C.c_void_p), ("lc_tgtfd", C.c_void_p), ("lc_nidx", C.c_int),
+        ("cen_l", C.c_double), ("cen_alpha", C.c_double),
+        ("rt_l", C.c_double), ("rt_wgt", C.c_void_p), ("rt_nwgt", C.c_int),
+        ("ri_l", C.c_double), ("ri_wgt", C.c_void_p), ("ri_nwgt", C.c_int),
+        ("rs_l", C.c_double), ("rs_wgt", C.c_void_p), ("rs_nwgt", C.c_int),
+        ("rf_l", C.c_double), ("rf_wgt", C.c_void_p), ("rf_nwgt", C.c_int),
+        ("isfcv", C.c_int), ("nfcv", C.c_int), ("uvidxfcv", C.c_void_p), ("vfcvr", C.c_void_p),
+        ("vfcvi", C.c_void_p), ("varfcv", C.c_void_p), ("wfcv", C.c_double),
+        ("isamp", C.c_int), ("namp", C.c_int), ("uvidxamp", C.c_void_p), ("vamp", C.c_void_p),
+        ("varamp", C.c_void_p), ("wamp", C.c_double),
+        ("iscp", C.c_int), ("ncp", C.c_int), ("uvidxcp", C.c_void_p), ("cp", C.c_void_p),
+        ("varcp", C.c_void_p), ("wcp", C.c_double),
+        ("isca", C.c_int), ("nca", C.c_int), ("uvidxca", C.c_void_p), ("ca", C.c_void_p),
+        ("varca", C.c_void_p), ("wca", C.c_double),
+        ("inormfactr", C.c_double),
+    ]
+
+
 class SolveInfo(C.Structure):
     _fields_ = [("task", C.c_int), ("niter", C.c_int), ("nfg", C.c_int), ("error", C.c_int)]
 
 
 TERM_NAMES = ["chisq", "chisqfcv", "chisqamp", "chisqcp", "chisqca", "reg", "l1_cost", "tv_cost",
               "tsv_cost", "kl_cost", "gs_cost", "tfd_cost", "cen_cost", "sm_cost", "cost"]
+TERM_NAMES_3D = ["chisq", "chisqfcv", "chisqamp", "chisqcp", "chisqca", "reg", "l1_cost", "sm_cost",
+                 "tv_cost", "tsv_cost", "kl_cost", "gs_cost", "tfd_cost", "lc_cost", "cen_cost",
+                 "rt_cost", "ri_cost", "rs_cost", "rf_cost", "cost"]
 TASK_CONV, TASK_ABNORMAL, TASK_STOP, TASK_ERROR, TASK_TARGET = 3, 4, 5, 6, 8
 
 EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "smili_batch_run",
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
            "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile",
-           "smili_batch_set_targets", "smili_calc_cost_noalloc"]
+           "smili_batch_set_targets", "smili_calc_cost_noalloc", "smili_fftim3d_imaging",
+           "smili_calc_cost3d"]
 STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
           "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
           "c_gather", "c_sort", "c_scan", "c_rounds"]
@@ -87,6 +123,9 @@ def lib():
                                             C.c_double, vp, dp, dp, vp]
         L.smili_calc_cost.argtypes = [vp, dp, vp, dp, dp]
         L.smili_calc_cost_noalloc.argtypes = [vp, dp, vp, dp, dp]
+        L.smili_fftim3d_imaging.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                            C.c_double, vp, dp, dp, vp]
+        L.smili_calc_cost3d.argtypes = [vp, dp, vp, dp, dp]
         L.smili_batch_create.argtypes = [C.c_int, C.POINTER(vp), ip, C.c_int, C.c_int, C.c_double,
                                          C.c_double, vp, C.POINTER(vp)]
         L.smili_batch_run.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]
@@ -162,6 +201,50 @@ class Problem:
     @property
     def npix(self):
         return self.c.npix
+
+
+class Movie:
+    """Contiguous copies of the fftim3d.imaging keyword arrays and the
+    ``smili_imaging3d_args`` struct that points into them."""
+
+    F64 = ["iin", "u", "v", "l1_wgt", "tv_wgt", "tsv_wgt", "kl_wgt", "gs_wgt", "lc_l", "lc_tgtfd", "rt_wgt",
+           "ri_wgt", "rs_wgt", "rf_wgt", "vfcvr", "vfcvi", "varfcv", "vamp", "varamp", "cp", "varcp", "ca",
+           "varca"]
+    I32 = ["xidx", "yidx", "uvidxfcv", "uvidxamp", "nuvs"]
+    SCAL = ["l1_l", "sm_l", "sm_maj", "sm_min", "sm_phi", "tv_l", "tsv_l", "kl_l", "gs_l", "tfd_l", "tfd_tgtfd",
+            "cen_l", "cen_alpha", "rt_l", "ri_l", "rs_l", "rf_l", "wfcv", "wamp", "wcp", "wca", "inormfactr"]
+
+    def __init__(self, kw: dict):
+        self.kw = kw
+        self.keep = {}
+        a = ImagingArgs3D()
+        for k in self.F64:
+            self.keep[k] = np.ascontiguousarray(np.asarray(kw[k], dtype=np.float64).reshape(-1))
+        for k in self.I32:
+            self.keep[k] = np.ascontiguousarray(np.asarray(kw[k], dtype=np.int32).reshape(-1))
+        self.keep["uvidxcp"] = np.ascontiguousarray(np.asarray(kw["uvidxcp"], dtype=np.int32).T).reshape(-1)
+        self.keep["uvidxca"] = np.ascontiguousarray(np.asarray(kw["uvidxca"], dtype=np.int32).T).reshape(-1)
+        for k, arr in self.keep.items():
+            setattr(a, k, arr.ctypes.data)
+        a.npix = int(kw["npix"])
+        a.nx, a.ny, a.nz = int(kw["nx"]), int(kw["ny"]), int(kw["nz"])
+        a.nxref, a.nyref = float(kw["nxref"]), float(kw["nyref"])
+        a.nuv = self.keep["u"].size
+        for k in self.SCAL:
+            setattr(a, k, float(kw[k]))
+        for k in ["l1", "tv", "tsv", "kl", "gs", "rt", "ri", "rs", "rf"]:
+            setattr(a, k + "_nwgt", int(kw[k + "_nwgt"]))
+        a.lc_nidx = int(kw["lc_nidx"])
+        a.isfcv, a.isamp, a.iscp, a.isca = (int(bool(kw[k])) for k in ["isfcv", "isamp", "iscp", "isca"])
+        a.nfcv = self.keep["uvidxfcv"].size
+        a.namp = self.keep["uvidxamp"].size
+        a.ncp = self.keep["uvidxcp"].size // 3
+        a.nca = self.keep["uvidxca"].size // 4
+        self.c = a
+
+    @property
+    def n(self):
+        return self.c.npix * self.c.nz
 
 
 class Batch:

@@ -569,8 +569,27 @@ __device__ void reg_moments(const ProbDesc& P, const double (&m)[10], RegMoments
   r.cen_cost = sqrt(r.cen_sx * r.cen_sx + r.cen_sy * r.cen_sy + 1e-10);
 }
 
+// image moments of a movie frame that has no data (the row pass of F1
+// accumulates the same sums for frames with data); one CTA, per-thread partials
+__device__ void frame_moments(const ProbDesc& P, char* base, double (&mom)[10]) {
+  const double* x = at<double>(base, P.o_x);
+  const int* xi = at<int>(base, P.o_xidx);
+  const int* yi = at<int>(base, P.o_yidx);
+  for (int p = threadIdx.x; p < P.npix; p += blockDim.x) {
+    const double val = x[p], fx = xi[p] + 1, fy = yi[p] + 1;
+    mom[0] += val;
+    mom[1] += fabs(val);
+    mom[2] += val * fx;
+    mom[3] += val * fy;
+    mom[4] += val * fx * fx;
+    mom[5] += val * fy * fy;
+    mom[6] += val * fx * fy;
+  }
+}
+
 __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, const RegMoments& rm,
-                            int lo, int hi, double (&reg)[8], double& gd, double& sbg) {
+                            int lo, int hi, double (&reg)[8], double& gd, double& sbg,
+                            bool opt_terms = true) {
   const double* x = at<double>(base, P.o_x);
   const int* inv = at<int>(base, P.o_inv);
   const int* xi = at<int>(base, P.o_xidx);
@@ -641,6 +660,7 @@ __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, co
     }
     const double gv = gchi[(size_t)iy * nx + ix] + gr;
     gout[p] = gv;
+    if (!opt_terms) continue;  // a movie frame: the movie pass forms g.d and the projected gradient
     gd += gv * d[p];
     // projected gradient (projgr, lbfgsb.f:2942-2990) with lower bound 0
     double gi = gv;

@@ -10,6 +10,7 @@
 #define SMILI_MAXM 8          // largest L-BFGS-B memory supported on the device
 #define SMILI_MAXW 16         // largest ES kernel width
 #define SMILI_NTERMS 15       // chisq, chisqfcv, chisqamp, chisqcp, chisqca, reg, l1..sm, cost
+#define SMILI_NTERMS3D 20     // a movie: ..., reg, l1, sm, tv, tsv, kl, gs, tfd, lc, cen, rt, ri, rs, rf, cost
 #define SMILI_NPART 16        // partial sums produced by one FG evaluation
 
 // data-term kinds in the flattened datum index space
@@ -40,6 +41,11 @@ struct ProbDesc {
   int has_l1, has_tv, has_tsv, has_kl, has_gs, has_tfd, has_cen, has_sm;
   int windowed;            // 1 when the pixel set is not the full nx*ny grid
   int nitems;              // spreading work items (<= 128 points of one 8x8 bin)
+  // movies (dynamic imaging): nframes >= 1 on a movie's descriptor (0 for a
+  // 2D problem), whose vectors hold npix = frame_npix * nframes values; each
+  // frame is a 2D descriptor (o_frames) whose x / g / d point into them
+  int nframes, frame_npix;
+  int has_rt, has_ri, has_lc;
   // scalars
   double beta;
   double wfcv, wamp, wcp, wca;       // normalised data weights (w / wtotal)
@@ -47,6 +53,7 @@ struct ProbDesc {
   double sm_l, sm_maj, sm_min, sm_phi;
   double nxref, nyref;
   double factr, pgtol;
+  double rt_l, ri_l;
   double ftarget;          // stop once f <= ftarget at a completed iteration (-inf: off)
   // byte offsets in the arena (0 = absent)
   int64_t o_x0, o_xidx, o_yidx, o_inv;
@@ -65,6 +72,8 @@ struct ProbDesc {
   int64_t o_sbk, o_sbi, o_hist;         // bucketed breakpoints, bucket counts/cursors
   int64_t o_cand, o_lred, o_state;
   int64_t o_trace;                      // cost at each NEW_X (double[niter+2])
+  int64_t o_frames;                     // movie: ProbDesc[nframes]
+  int64_t o_rtw, o_riw, o_lcf, o_iavg;  // movie: Rt / Ri weights, light curve, pixel average
   int64_t o_out;                        // results: terms[15], counters
 };
 
@@ -78,7 +87,7 @@ struct LbState {
   int nfg_total;
   double f, theta, fold, tol, dnorm, gd, gdold, stp, stpmx, sbgnrm, dtd, xstep, epsmch;
   double ginit, gtest, gx, gy, finit, fx, fy, stx, sty, stmin, stmax, width, width1;
-  double terms[SMILI_NTERMS];
+  double terms[SMILI_NTERMS3D];
   double sy[SMILI_MAXM * SMILI_MAXM], ss[SMILI_MAXM * SMILI_MAXM], wt[SMILI_MAXM * SMILI_MAXM];
   double wn[4 * SMILI_MAXM * SMILI_MAXM], wn1[4 * SMILI_MAXM * SMILI_MAXM];
   double wa[8 * SMILI_MAXM];
@@ -86,6 +95,6 @@ struct LbState {
 
 // per-problem results copied back to the host
 struct ProbResult {
-  double terms[SMILI_NTERMS];
+  double terms[SMILI_NTERMS3D];
   int task, iter, nfg, error;
 };

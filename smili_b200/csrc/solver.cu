@@ -46,6 +46,93 @@ struct BatchArgs {
 // ---------------------------------------------------------------------------
 // one function/gradient evaluation by the group (stages F1..F8)
 // ---------------------------------------------------------------------------
+// Stages F1-F8 of one evaluation of a 2D problem by group g: per-thread
+// partial sums acc[0..3] = chi-square terms (weighted), acc[4..11] = the
+// per-pixel regularizers (l1, tv, tsv, kl, gs, -, -, -), acc[12] = g.d,
+// acc[13] = projected-gradient max, and the image moments rm.  opt_terms
+// false leaves acc[12..13] alone (a movie frame).  A frame without data
+// (nuv == 0) only evaluates its regularizers.
+template <typename R>
+__device__ bool fg_stages(FgCtx<R>& fc, GroupCtx& g, int lo, int hi, double* red, unsigned char* ops,
+                          double* scratch, double (&acc)[16], RegMoments& rm, int mode, bool opt_terms,
+                          Prof& pf) {
+  const ProbDesc& P = *fc.P;
+  memset(&rm, 0, sizeof(rm));
+  double chi[4] = {0, 0, 0, 0};
+  if (P.nuv > 0) {
+    double mom[10];
+    for (int k = 0; k < 10; ++k) mom[k] = 0.0;
+    fg_t2_rows(fc, g, mom);
+    if (P.has_tfd || P.has_cen || P.has_sm) {
+      for (int k = threadIdx.x; k < 10; k += blockDim.x) ops[k] = RED_SUM;
+      __syncthreads();
+      block_reduce_arr(mom, ops, 10, red, scratch);
+      if (!group_reduce(g, red, ops, 10)) return false;
+      double mm[10];
+      for (int k = 0; k < 10; ++k) mm[k] = red[k];
+      reg_moments(P, mm, rm);
+      __syncthreads();
+    } else if (!group_sync(g)) {
+      return false;
+    }
+    pf.mark(PR_F1);
+    fg_t2_cols(fc, g);
+    if (!group_sync(g)) return false;
+    pf.mark(PR_F2);
+    fg_interp(fc, g);
+    if (!group_sync(g)) return false;
+    pf.mark(PR_F3);
+    if (mode == MODE_T2) return true;
+    if (mode != MODE_T1) {
+      fg_chisq(fc, g, chi);
+      if (!group_sync(g)) return false;
+    }
+    pf.mark(PR_F4);
+    fg_spread(fc, g);
+    if (!group_sync(g)) return false;
+    pf.mark(PR_F5);
+    fg_t1_rows(fc, g);
+    if (!group_sync(g)) return false;
+    pf.mark(PR_F6);
+    fg_t1_cols(fc, g);
+    if (!group_sync(g)) return false;
+    pf.mark(PR_F7);
+    if (mode == MODE_T1) return true;
+  } else if (P.has_tfd || P.has_sm) {
+    double mom[10];
+    for (int k = 0; k < 10; ++k) mom[k] = 0.0;
+    frame_moments(P, fc.base, mom);
+    for (int k = threadIdx.x; k < 10; k += blockDim.x) ops[k] = RED_SUM;
+    __syncthreads();
+    block_reduce_arr(mom, ops, 10, red, scratch);
+    double mm[10];
+    for (int k = 0; k < 10; ++k) mm[k] = red[k];
+    reg_moments(P, mm, rm);
+    __syncthreads();
+  }
+  double reg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  fg_reg_grad(P, fc.base, g, rm, lo, hi, reg, acc[12], acc[13], opt_terms);
+  for (int k = 0; k < 4; ++k) acc[k] += chi[k];
+  for (int k = 0; k < 8; ++k) acc[4 + k] += reg[k];
+  return true;
+}
+
+// global-sum regularizers of one 2D image (image.f90:108-135) from its moments
+__device__ __forceinline__ void global_regs(const ProbDesc& P, const RegMoments& rm, double& tfd, double& cen,
+                                            double& sm) {
+  tfd = P.has_tfd ? P.tfd_l * rm.tfd_resid * rm.tfd_resid : 0.0;
+  cen = P.has_cen ? P.cen_l * rm.cen_cost : 0.0;
+  sm = 0.0;
+  if (P.has_sm) {
+    double e = 0;
+    for (int q = 0; q < 2; ++q) e += (rm.Sg[q] - rm.Sp[q]) * (rm.Sg[q] - rm.Sp[q]);
+    e += 2. * (rm.Sg[2] - rm.Sp[2]) * (rm.Sg[2] - rm.Sp[2]);
+    sm = P.sm_l * e;
+  }
+}
+
+// One evaluation of a 2D problem: f, g.d, projected-gradient norm and the
+// 15 cost terms (fftim2d.f90:387-607).
 template <typename R>
 __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsigned char* ops,
                          double* scratch, double& f, double& gd, double& sbg, double* terms,
@@ -53,53 +140,11 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
   const ProbDesc& P = *fc.P;
   Prof& pf = *lc.prof;
   pf.mark(PR_OTHER);
-  double mom[10];
-  for (int k = 0; k < 10; ++k) mom[k] = 0.0;
-  fg_t2_rows(fc, g, mom);
+  double acc[16];
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
   RegMoments rm;
-  memset(&rm, 0, sizeof(rm));
-  if (P.has_tfd || P.has_cen || P.has_sm) {
-    for (int k = threadIdx.x; k < 10; k += blockDim.x) ops[k] = RED_SUM;
-    __syncthreads();
-    block_reduce_arr(mom, ops, 10, red, scratch);
-    if (!group_reduce(g, red, ops, 10)) return false;
-    double mm[10];
-    for (int k = 0; k < 10; ++k) mm[k] = red[k];
-    reg_moments(P, mm, rm);
-    __syncthreads();
-  } else if (!group_sync(g)) {
-    return false;
-  }
-  pf.mark(PR_F1);
-  fg_t2_cols(fc, g);
-  if (!group_sync(g)) return false;
-  pf.mark(PR_F2);
-  fg_interp(fc, g);
-  if (!group_sync(g)) return false;
-  pf.mark(PR_F3);
-  if (mode == MODE_T2) return true;
-  double chi[4] = {0, 0, 0, 0};
-  if (mode != MODE_T1) {
-    fg_chisq(fc, g, chi);
-    if (!group_sync(g)) return false;
-  }
-  pf.mark(PR_F4);
-  fg_spread(fc, g);
-  if (!group_sync(g)) return false;
-  pf.mark(PR_F5);
-  fg_t1_rows(fc, g);
-  if (!group_sync(g)) return false;
-  pf.mark(PR_F6);
-  fg_t1_cols(fc, g);
-  if (!group_sync(g)) return false;
-  pf.mark(PR_F7);
-  if (mode == MODE_T1) return true;
-  double acc[14];
-  for (int k = 0; k < 14; ++k) acc[k] = 0.0;
-  double reg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  fg_reg_grad(P, fc.base, g, rm, lc.lo, lc.hi, reg, acc[12], acc[13]);
-  for (int k = 0; k < 4; ++k) acc[k] = chi[k];
-  for (int k = 0; k < 8; ++k) acc[4 + k] = reg[k];
+  if (!fg_stages(fc, g, lc.lo, lc.hi, red, ops, scratch, acc, rm, mode, true, pf)) return false;
+  if (mode == MODE_T1 || mode == MODE_T2) return true;
   for (int k = threadIdx.x; k < 14; k += blockDim.x) ops[k] = (k == 13) ? RED_MAX : RED_SUM;
   __syncthreads();
   block_reduce_arr(acc, ops, 14, red, scratch);
@@ -109,15 +154,7 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
   __syncthreads();
   pf.mark(PR_F8);
   pf.count(PR_COUNT);
-  // global-sum regularizers (image.f90:108-135)
-  if (P.has_tfd) r[4 + 5] = P.tfd_l * rm.tfd_resid * rm.tfd_resid;
-  if (P.has_cen) r[4 + 6] = P.cen_l * rm.cen_cost;
-  if (P.has_sm) {
-    double e = 0;
-    for (int q = 0; q < 2; ++q) e += (rm.Sg[q] - rm.Sp[q]) * (rm.Sg[q] - rm.Sp[q]);
-    e += 2. * (rm.Sg[2] - rm.Sp[2]) * (rm.Sg[2] - rm.Sp[2]);
-    r[4 + 7] = P.sm_l * e;
-  }
+  global_regs(P, rm, r[4 + 5], r[4 + 6], r[4 + 7]);
   const double chisq = r[0] + r[1] + r[2] + r[3];
   double regs = 0;
   for (int k = 0; k < 8; ++k) regs += r[4 + k];
@@ -133,6 +170,120 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
     terms[5] = regs;
     for (int k = 0; k < 8; ++k) terms[6 + k] = r[4 + k];
     terms[14] = f;
+  }
+  __syncthreads();
+  return true;
+}
+
+// One evaluation of a movie (fftim3d.f90:473-614, fftlib3d.f90:14-205,
+// image3d.f90:15-425).  Every frame is a complete 2D evaluation run by one
+// CTA (frames z = rank, rank + G, ...) with the frame's regularizer weights
+// already divided by the frame count; after a group barrier the movie pass
+// adds the Rt / Ri gradients (image3d.f90:280-392, Rt only for frames
+// iz < Nz as the reference does) and forms g.d and the projected gradient
+// over the whole vector.  terms[20] follow the fftim3d.imaging order.
+template <typename R>
+__device__ bool movie_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsigned char* ops,
+                         double* scratch, double& f, double& gd, double& sbg, double* terms) {
+  const ProbDesc& M = *fc.P;
+  char* base = fc.base;
+  Prof& pf = *lc.prof;
+  pf.mark(PR_OTHER);
+  const ProbDesc* frames = at<ProbDesc>(base, M.o_frames);
+  double acc[16];
+  for (int k = 0; k < 16; ++k) acc[k] = 0.0;
+  GroupCtx g1 = g;  // one CTA per frame: G == 1 barriers are block barriers
+  g1.rank = 0;
+  g1.G = 1;
+  for (int z = g.rank; z < M.nframes; z += g.G) {
+    FgCtx<R> fz = fc;
+    fz.P = &frames[z];
+    RegMoments rm;
+    if (!fg_stages(fz, g1, 0, frames[z].npix, red, ops, scratch, acc, rm, MODE_FG, false, pf)) return false;
+    if (threadIdx.x == 0) {
+      double tfd, cen, sm;
+      global_regs(frames[z], rm, tfd, cen, sm);
+      acc[4 + 5] += tfd;  // the light-curve term when M.has_lc
+      acc[4 + 7] += sm;
+    }
+    __syncthreads();
+  }
+  if (!group_sync(g)) return false;
+  const int N = M.frame_npix, Nz = M.nframes;
+  const double* x = lc.x;
+  double* gv = lc.gv;
+  const double* d = lc.d;
+  const double* lcf = at<double>(base, M.o_lcf);
+  double* iavg = M.has_ri ? at<double>(base, M.o_iavg) : nullptr;
+  if (M.has_ri) {
+    const int chunk = (N + g.G - 1) / g.G;
+    const int p0 = min(N, g.rank * chunk), p1 = min(N, p0 + chunk);
+    for (int i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+      double s = 0.0;
+      for (int z = 0; z < Nz; ++z) s += x[(size_t)z * N + i] / lcf[z] / Nz;
+      iavg[i] = s;
+    }
+    if (!group_sync(g)) return false;
+  }
+  const double* rtw = M.has_rt ? at<double>(base, M.o_rtw) : nullptr;
+  const double* riw = M.has_ri ? at<double>(base, M.o_riw) : nullptr;
+  for (int idx = lc.lo + threadIdx.x; idx < lc.hi; idx += blockDim.x) {
+    const int z = idx / N, i = idx - z * N;
+    const double II = x[idx] / lcf[z];
+    double gr = 0.0;
+    if (M.has_rt && z + 1 < Nz) {
+      const double Iu = x[idx + N] / lcf[z + 1];
+      acc[14] += M.rt_l * rtw[i] * (Iu - II) * (Iu - II);
+      const double ge = (z == 0) ? 2.0 * (II - Iu) : 2.0 * (2.0 * II - x[idx - N] / lcf[z - 1] - Iu);
+      gr += M.rt_l * rtw[i] * ge / lcf[z];
+    }
+    if (M.has_ri) {
+      acc[15] += M.ri_l * riw[i] * (II - iavg[i]) * (II - iavg[i]);
+      gr += M.ri_l * riw[i] * 2.0 * (II - iavg[i]) / lcf[z];
+    }
+    const double gi_full = gv[idx] + gr;
+    gv[idx] = gi_full;
+    acc[12] += gi_full * d[idx];
+    double gi = gi_full;
+    if (M.nonneg && gi >= 0.0) gi = fmin(x[idx], gi);
+    acc[13] = fmax(acc[13], fabs(gi));
+  }
+  for (int k = threadIdx.x; k < 16; k += blockDim.x) ops[k] = (k == 13) ? RED_MAX : RED_SUM;
+  __syncthreads();
+  block_reduce_arr(acc, ops, 16, red, scratch);
+  if (!group_reduce(g, red, ops, 16)) return false;
+  double r[16];
+  for (int k = 0; k < 16; ++k) r[k] = red[k];
+  __syncthreads();
+  pf.mark(PR_F8);
+  pf.count(PR_COUNT);
+  const double chisq = r[0] + r[1] + r[2] + r[3];
+  double regs = r[14] + r[15];
+  for (int k = 0; k < 8; ++k) regs += r[4 + k];
+  f = chisq + regs;
+  gd = r[12];
+  sbg = r[13];
+  if (threadIdx.x == 0) {
+    terms[0] = chisq;
+    terms[1] = M.nfcv ? r[0] / M.wfcv / (2.0 * M.nfcv) : 0.0;
+    terms[2] = M.namp ? r[1] / M.wamp / M.namp : 0.0;
+    terms[3] = M.ncp ? r[2] / M.wcp / M.ncp : 0.0;
+    terms[4] = M.nca ? r[3] / M.wca / M.nca : 0.0;
+    terms[5] = regs;
+    terms[6] = r[4];                        // l1
+    terms[7] = r[4 + 7];                    // sm
+    terms[8] = r[5];                        // tv
+    terms[9] = r[6];                        // tsv
+    terms[10] = r[7];                       // kl
+    terms[11] = r[8];                       // gs
+    terms[12] = M.has_lc ? 0.0 : r[4 + 5];  // tfd
+    terms[13] = M.has_lc ? r[4 + 5] : 0.0;  // lc
+    terms[14] = 0.0;                        // cen (not evaluated for movies)
+    terms[15] = r[14];                      // rt
+    terms[16] = r[15];                      // ri
+    terms[17] = 0.0;                        // rs (not evaluated by the reference)
+    terms[18] = 0.0;                        // rf (not evaluated by the reference)
+    terms[19] = f;
   }
   __syncthreads();
   return true;
@@ -235,10 +386,11 @@ __global__ void __launch_bounds__(SMILI_THREADS, sizeof(R) == 4 ? 3 : 2) smili_b
     }
     bool ok = group_sync(g);
     prof.mark(PR_INIT);
-    double terms_l[SMILI_NTERMS];
     while (ok) {
       double f = 0, gd = 0, sbg = 0;
-      if (!group_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms, a.mode)) {
+      const bool okf = P.nframes > 0 ? movie_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms)
+                                     : group_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms, a.mode);
+      if (!okf) {
         ok = false;
         break;
       }
@@ -256,14 +408,15 @@ __global__ void __launch_bounds__(SMILI_THREADS, sizeof(R) == 4 ? 3 : 2) smili_b
       // final summary evaluation at the returned image (fftim2d.f90:356-376)
       if (!group_sync(g)) ok = false;
       double f = 0, gd = 0, sbg = 0;
-      if (ok && !group_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms, MODE_FG)) ok = false;
+      if (ok && !(P.nframes > 0 ? movie_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms)
+                                : group_fg<R>(fc, g, lc, red, ops, scratch, f, gd, sbg, S.terms, MODE_FG)))
+        ok = false;
       if (threadIdx.x == 0) S.nfg_total++;
     }
-    (void)terms_l;
     __syncthreads();
     if (rank == 0 && threadIdx.x == 0) {
       ProbResult& res = a.results[p];
-      for (int k = 0; k < SMILI_NTERMS; ++k) res.terms[k] = S.terms[k];
+      for (int k = 0; k < SMILI_NTERMS3D; ++k) res.terms[k] = S.terms[k];
       res.task = ok ? S.task : LB_TASK_ERROR;
       res.iter = S.iter;
       res.nfg = S.nfg_total;
@@ -392,16 +545,17 @@ struct HostProb {
   }
 };
 
-enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3 };
+enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4 };  // PK_FRAME: one frame of a movie
 
 template <typename R>
 int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, int m, double factr,
                  double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override,
-                 const double* c_re, const double* c_im) {
+                 const double* c_re, const double* c_im, double wtotal_override = 0.0) {
   ProbDesc& d = hp.d;
   std::memset(&d, 0, sizeof(d));
   const int N = a.npix, nx = a.nx, ny = a.ny, nuv = a.nuv;
-  if (N < 1 || nx < 1 || ny < 1 || nuv < 1 || (long)N > (long)nx * ny)
+  const bool frame = kind == PK_FRAME;  // x / g / d live in the movie's vectors; data weights are global
+  if (N < 1 || nx < 1 || ny < 1 || nuv < (frame ? 0 : 1) || (long)N > (long)nx * ny)
     return fail(SMILI_ERR_ARG, "invalid image or uv sizes");
   if (m < 1 || m > SMILI_MAXM_DEV) return fail(SMILI_ERR_UNSUPPORTED, "L-BFGS-B memory m must be 1..6");
   if (!a.iin || !a.xidx || !a.yidx || !a.u || !a.v) return fail(SMILI_ERR_ARG, "null array");
@@ -443,12 +597,12 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.nyref = a.nyref;
   d.windowed = N != nx * ny;
   // data terms
-  const bool use_data = kind == PK_SOLVE || kind == PK_FG;
+  const bool use_data = kind == PK_SOLVE || kind == PK_FG || frame;
   const int nfcv = (use_data && a.isfcv) ? a.nfcv : 0;
   const int namp = (use_data && a.isamp) ? a.namp : 0;
   const int ncp = (use_data && a.iscp) ? a.ncp : 0;
   const int nca = (use_data && a.isca) ? a.nca : 0;
-  if (use_data && nfcv + namp + ncp + nca == 0) return fail(SMILI_ERR_ARG, "no data terms");
+  if (use_data && nuv > 0 && nfcv + namp + ncp + nca == 0) return fail(SMILI_ERR_ARG, "no data terms");
   d.nfcv = nfcv;
   d.namp = namp;
   d.ncp = ncp;
@@ -462,12 +616,13 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   if (namp) wtotal += (double)namp * a.wamp;
   if (ncp) wtotal += (double)ncp * a.wcp;
   if (nca) wtotal += (double)nca * a.wca;
+  if (wtotal_override > 0) wtotal = wtotal_override;  // a movie frame: the whole movie's data
   d.wfcv = nfcv ? a.wfcv / wtotal : 0;
   d.wamp = namp ? a.wamp / wtotal : 0;
   d.wcp = ncp ? a.wcp / wtotal : 0;
   d.wca = nca ? a.wca / wtotal : 0;
   // regularizers (active when lambda > 0, image.f90:112-175)
-  const bool use_reg = kind == PK_SOLVE || kind == PK_FG;
+  const bool use_reg = kind == PK_SOLVE || kind == PK_FG || frame;
   auto need_w = [&](double l, const double* wv, int nw, const char* nm) -> int {
     if (!(use_reg && l > 0)) return 0;
     if (!wv || nw != N) return fail(SMILI_ERR_ARG, std::string(nm) + " weights must have npix entries");
@@ -501,6 +656,28 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.sm_maj = a.sm_maj;
   d.sm_min = a.sm_min;
   d.sm_phi = a.sm_phi;
+  if (frame && nuv == 0) {
+    // a movie frame without data: pixel maps, regularizer weights and a
+    // zero chi-square gradient (the arena is cleared at upload)
+    d.o_xidx = ar.take(sizeof(int) * N);
+    d.o_yidx = ar.take(sizeof(int) * N);
+    d.o_inv = ar.take(sizeof(int) * (size_t)nx * ny);
+    if (d.has_l1) d.o_l1w = ar.take(sizeof(double) * N);
+    if (d.has_tv) d.o_tvw = ar.take(sizeof(double) * N);
+    if (d.has_tsv) d.o_tsvw = ar.take(sizeof(double) * N);
+    if (d.has_kl) d.o_klw = ar.take(sizeof(double) * N);
+    if (d.has_gs) d.o_gsw = ar.take(sizeof(double) * N);
+    d.o_gchi = ar.take(sizeof(double) * (size_t)nx * ny);
+    hp.put(d.o_xidx, xi);
+    hp.put(d.o_yidx, yi);
+    hp.put(d.o_inv, inv);
+    if (d.has_l1) hp.put(d.o_l1w, std::vector<double>(a.l1_wgt, a.l1_wgt + N));
+    if (d.has_tv) hp.put(d.o_tvw, std::vector<double>(a.tv_wgt, a.tv_wgt + N));
+    if (d.has_tsv) hp.put(d.o_tsvw, std::vector<double>(a.tsv_wgt, a.tsv_wgt + N));
+    if (d.has_kl) hp.put(d.o_klw, std::vector<double>(a.kl_wgt, a.kl_wgt + N));
+    if (d.has_gs) hp.put(d.o_gsw, std::vector<double>(a.gs_wgt, a.gs_wgt + N));
+    return SMILI_OK;
+  }
 
   // fine-grid coordinates in the kernel precision, band of touched cells
   std::vector<R> xu(nuv), xv(nuv);
@@ -660,7 +837,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   };
   // ---- arena layout ----
   const size_t C = sizeof(cpx<R>);
-  d.o_x0 = ar.take(sizeof(double) * N);
+  if (!frame) d.o_x0 = ar.take(sizeof(double) * N);
   d.o_xidx = ar.take(sizeof(int) * N);
   d.o_yidx = ar.take(sizeof(int) * N);
   d.o_inv = ar.take(sizeof(int) * (size_t)nx * ny);
@@ -690,8 +867,10 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.o_bandC = ar.take(C * (size_t)d.b2n * d.b1n);
   d.o_tmpC = ar.take(C * (size_t)d.b2n * nx);
   d.o_gchi = ar.take(sizeof(double) * (size_t)nx * ny);
-  d.o_x = ar.take(sizeof(double) * N);
-  d.o_g = ar.take(sizeof(double) * N);
+  if (!frame) {
+    d.o_x = ar.take(sizeof(double) * N);
+    d.o_g = ar.take(sizeof(double) * N);
+  }
   if (kind == PK_SOLVE || kind == PK_FG) {
     d.o_z = ar.take(sizeof(double) * N);
     d.o_r = ar.take(sizeof(double) * N);
@@ -712,7 +891,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.o_wy = ar.take(sizeof(double) * (size_t)N * m);
   }
   // ---- blobs ----
-  hp.put(d.o_x0, std::vector<double>(x0, x0 + N));
+  if (!frame) hp.put(d.o_x0, std::vector<double>(x0, x0 + N));
   hp.put(d.o_xidx, xi);
   hp.put(d.o_yidx, yi);
   hp.put(d.o_inv, inv);
@@ -737,7 +916,8 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   hp.put(d.o_items, items);
   if (kind == PK_T1) hp.put(d.o_contrib, contrib0);
   // the original -> sorted uv permutation is needed to return visibilities
-  hp.blobs.emplace_back(-1, std::vector<char>((const char*)perm.data(), (const char*)perm.data() + sizeof(int) * nuv));
+  if (!frame)
+    hp.blobs.emplace_back(-1, std::vector<char>((const char*)perm.data(), (const char*)perm.data() + sizeof(int) * nuv));
   return SMILI_OK;
 }
 
@@ -815,6 +995,10 @@ int launch_batch(smili_batch* b, int mode, float* ms) {
 }
 
 template <typename R>
+int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smili_options* opt,
+                 smili_batch** out);
+
+template <typename R>
 int create_batch(int nprob, const smili_imaging_args* const* probs, const int* niter, int nonneg,
                  int m, double factr, double pgtol, const smili_options* opt, int kind,
                  const double* const* x_over, const double* c_re, const double* c_im,
@@ -841,6 +1025,16 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
     maxn = std::max(maxn, hps[p].d.npix);
   }
   b->arena_bytes = ar.bytes;
+  return finish_batch<R>(b, hps, maxn, opt, out);
+}
+
+// Device side of a batch whose problems are packed (descs, arena size, host
+// blobs): launch geometry, buffers, upload.  Takes ownership of b.
+template <typename R>
+int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smili_options* opt,
+                 smili_batch** out) {
+  const int device = b->device;
+  const int nprob = b->nprob;
   // inputs are valid: now the device
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) {
@@ -928,6 +1122,296 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   return SMILI_OK;
 }
 
+// Pack one movie (fftim3d): the movie's descriptor carries the optimiser
+// vectors over npix * nz values and the Rt / Ri / light-curve arrays; every
+// frame is packed as a 2D problem (PK_FRAME) over its own slice of the uv
+// list and its own data, with the whole movie's data weights, the static
+// regularizers divided by nz (image3d.f90:219-257; per-frame weights scaled
+// by the light curve when lc_nidx is 1 or 3, image3d.f90:188-200) and the
+// centroid term off (image3d.f90:210); its x / g / d point into the
+// movie's vectors.
+template <typename R>
+int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, int m, double factr,
+               double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override) {
+  const int N = a.npix, Nz = a.nz, nuv = a.nuv;
+  if (N < 1 || Nz < 1 || nuv < 0 || a.nx < 1 || a.ny < 1 || (long)N * Nz > 0x7fffffffL)
+    return fail(SMILI_ERR_ARG, "invalid movie sizes");
+  if (!a.iin || !a.xidx || !a.yidx || !a.nuvs || !a.lc_l || !a.lc_tgtfd || (nuv > 0 && (!a.u || !a.v)))
+    return fail(SMILI_ERR_ARG, "null movie array");
+  std::vector<int> off(Nz + 1, 0);
+  for (int z = 0; z < Nz; ++z) {
+    if (a.nuvs[z] < 0) return fail(SMILI_ERR_ARG, "negative nuvs");
+    off[z + 1] = off[z] + a.nuvs[z];
+  }
+  if (off[Nz] != nuv) return fail(SMILI_ERR_ARG, "nuvs does not add up to nuv");
+  for (int z = 0; z < Nz; ++z)
+    if (!(a.lc_tgtfd[z] != 0.0) || !std::isfinite(a.lc_tgtfd[z]))
+      return fail(SMILI_ERR_DATA, "lc_tgtfd must be finite and nonzero");
+  const int nfcv = a.isfcv ? a.nfcv : 0, namp = a.isamp ? a.namp : 0, ncp = a.iscp ? a.ncp : 0,
+            nca = a.isca ? a.nca : 0;
+  double wtotal = 0;
+  if (nfcv) wtotal += 2.0 * nfcv * a.wfcv;
+  if (namp) wtotal += (double)namp * a.wamp;
+  if (ncp) wtotal += (double)ncp * a.wcp;
+  if (nca) wtotal += (double)nca * a.wca;
+  if (!(wtotal > 0)) return fail(SMILI_ERR_ARG, "no data terms");
+  auto frame_of = [&](int idx, int& z, int& local) -> int {
+    const int k = std::abs(idx) - 1;
+    if (idx == 0 || k >= nuv) return fail(SMILI_ERR_ARG, "uv index out of range");
+    z = (int)(std::upper_bound(off.begin(), off.end(), k) - off.begin()) - 1;
+    local = (idx > 0 ? 1 : -1) * (k - off[z] + 1);
+    return SMILI_OK;
+  };
+  // split the data by frame (frame-local signed uv indices)
+  struct FrameData {
+    std::vector<int> ifcv, iamp, icp, ica;
+    std::vector<double> fr, fi, fv, av, avar, cpv, cpvar, cav, cavar;
+  };
+  std::vector<FrameData> fd(Nz);
+  int rc;
+  for (int i = 0; i < nfcv; ++i) {
+    int z, l;
+    if ((rc = frame_of(a.uvidxfcv[i], z, l)) < 0) return rc;
+    fd[z].ifcv.push_back(l);
+    fd[z].fr.push_back(a.vfcvr[i]);
+    fd[z].fi.push_back(a.vfcvi[i]);
+    fd[z].fv.push_back(a.varfcv[i]);
+  }
+  for (int i = 0; i < namp; ++i) {
+    int z, l;
+    if ((rc = frame_of(a.uvidxamp[i], z, l)) < 0) return rc;
+    fd[z].iamp.push_back(l);
+    fd[z].av.push_back(a.vamp[i]);
+    fd[z].avar.push_back(a.varamp[i]);
+  }
+  for (int i = 0; i < ncp; ++i) {
+    int z0 = -1, ls[3];
+    for (int q = 0; q < 3; ++q) {
+      int z;
+      if ((rc = frame_of(a.uvidxcp[3 * i + q], z, ls[q])) < 0) return rc;
+      if (q && z != z0) return fail(SMILI_ERR_UNSUPPORTED, "a closure phase spans two frames");
+      z0 = z;
+    }
+    for (int q = 0; q < 3; ++q) fd[z0].icp.push_back(ls[q]);
+    fd[z0].cpv.push_back(a.cp[i]);
+    fd[z0].cpvar.push_back(a.varcp[i]);
+  }
+  for (int i = 0; i < nca; ++i) {
+    int z0 = -1, ls[4];
+    for (int q = 0; q < 4; ++q) {
+      int z;
+      if ((rc = frame_of(a.uvidxca[4 * i + q], z, ls[q])) < 0) return rc;
+      if (q && z != z0) return fail(SMILI_ERR_UNSUPPORTED, "a closure amplitude spans two frames");
+      z0 = z;
+    }
+    for (int q = 0; q < 4; ++q) fd[z0].ica.push_back(ls[q]);
+    fd[z0].cav.push_back(a.ca[i]);
+    fd[z0].cavar.push_back(a.varca[i]);
+  }
+  for (int z = 0; z < Nz; ++z)
+    if (a.nuvs[z] > 0 && fd[z].ifcv.empty() && fd[z].iamp.empty() && fd[z].icp.empty() && fd[z].ica.empty())
+      return fail(SMILI_ERR_ARG, "a frame has uv points but no data");
+  double lcsum = 0;
+  for (int z = 0; z < Nz; ++z) lcsum += a.lc_l[z];
+  const bool lc_on = lcsum > 0;
+  const bool lc_scale = lc_on && (a.lc_nidx == 1 || a.lc_nidx == 3);
+  const double* xsrc = x_override ? x_override : a.iin;
+  if (!finite_all(xsrc, N * Nz)) return fail(SMILI_ERR_DATA, "non-finite initial movie");
+  // movie descriptor and its vectors
+  ProbDesc& d = hp.d;
+  std::memset(&d, 0, sizeof(d));
+  const int n = N * Nz;
+  d.npix = n;
+  d.nx = a.nx;
+  d.ny = a.ny;
+  d.m = m;
+  d.niter = niter;
+  d.nonneg = nonneg ? 1 : 0;
+  d.factr = factr;
+  d.pgtol = pgtol;
+  d.ftarget = -INFINITY;
+  d.prec64 = sizeof(R) == 8;
+  d.nxref = a.nxref;
+  d.nyref = a.nyref;
+  d.nframes = Nz;
+  d.frame_npix = N;
+  d.nfcv = nfcv;
+  d.namp = namp;
+  d.ncp = ncp;
+  d.nca = nca;
+  d.wfcv = nfcv ? a.wfcv / wtotal : 0;
+  d.wamp = namp ? a.wamp / wtotal : 0;
+  d.wcp = ncp ? a.wcp / wtotal : 0;
+  d.wca = nca ? a.wca / wtotal : 0;
+  d.has_rt = a.rt_l > 0;
+  d.has_ri = a.ri_l > 0;
+  d.has_lc = lc_on;
+  d.rt_l = a.rt_l;
+  d.ri_l = a.ri_l;
+  if (d.has_rt && (!a.rt_wgt || a.rt_nwgt != N)) return fail(SMILI_ERR_ARG, "rt weights must have npix entries");
+  if (d.has_ri && (!a.ri_wgt || a.ri_nwgt != N)) return fail(SMILI_ERR_ARG, "ri weights must have npix entries");
+  d.o_x0 = ar.take(sizeof(double) * n);
+  d.o_x = ar.take(sizeof(double) * n);
+  d.o_g = ar.take(sizeof(double) * n);
+  d.o_z = ar.take(sizeof(double) * n);
+  d.o_r = ar.take(sizeof(double) * n);
+  d.o_d = ar.take(sizeof(double) * n);
+  d.o_t = ar.take(sizeof(double) * n);
+  d.o_xp = ar.take(sizeof(double) * n);
+  d.o_iwh = ar.take(n);
+  d.o_free = ar.take(n);
+  d.o_bkey = ar.take(sizeof(unsigned long long) * n);
+  d.o_sbk = ar.take(sizeof(unsigned long long) * n);
+  d.o_sbi = ar.take(sizeof(int) * n);
+  d.o_hist = ar.take(sizeof(int) * 2 * 4096);
+  d.o_lred = ar.take(sizeof(double) * 64);
+  d.o_trace = ar.take(sizeof(double) * (niter + 2));
+  if (kind == PK_SOLVE) {
+    d.o_ws = ar.take(sizeof(double) * (size_t)n * m);
+    d.o_wy = ar.take(sizeof(double) * (size_t)n * m);
+  }
+  d.o_frames = ar.take(sizeof(ProbDesc) * Nz);
+  d.o_lcf = ar.take(sizeof(double) * Nz);
+  if (d.has_rt) d.o_rtw = ar.take(sizeof(double) * N);
+  if (d.has_ri) {
+    d.o_riw = ar.take(sizeof(double) * N);
+    d.o_iavg = ar.take(sizeof(double) * N);
+  }
+  // frames
+  std::vector<HostProb> fh(Nz);
+  std::vector<double> w1, wtv, wtsv, wkl, wgs;
+  for (int z = 0; z < Nz; ++z) {
+    const FrameData& f = fd[z];
+    smili_imaging_args fa;
+    std::memset(&fa, 0, sizeof(fa));
+    fa.npix = N;
+    fa.nx = a.nx;
+    fa.ny = a.ny;
+    fa.iin = xsrc + (size_t)z * N;
+    fa.xidx = a.xidx;
+    fa.yidx = a.yidx;
+    fa.nxref = a.nxref;
+    fa.nyref = a.nyref;
+    fa.nuv = a.nuvs[z];
+    fa.u = nuv ? a.u + off[z] : nullptr;
+    fa.v = nuv ? a.v + off[z] : nullptr;
+    const double c = lc_scale ? a.tfd_tgtfd / a.lc_tgtfd[z] : 1.0;
+    auto scaled = [&](const double* w, int nw, double fac, std::vector<double>& buf) -> const double* {
+      if (!w || fac == 1.0) return w;
+      buf.assign(w, w + nw);
+      for (auto& v : buf) v *= fac;
+      return buf.data();
+    };
+    fa.l1_l = a.l1_l > 0 ? a.l1_l / Nz : a.l1_l;
+    fa.l1_wgt = scaled(a.l1_wgt, a.l1_nwgt, c, w1);
+    fa.l1_nwgt = a.l1_nwgt;
+    fa.tv_l = a.tv_l > 0 ? a.tv_l / Nz : a.tv_l;
+    fa.tv_wgt = scaled(a.tv_wgt, a.tv_nwgt, c, wtv);
+    fa.tv_nwgt = a.tv_nwgt;
+    fa.tsv_l = a.tsv_l > 0 ? a.tsv_l / Nz : a.tsv_l;
+    fa.tsv_wgt = scaled(a.tsv_wgt, a.tsv_nwgt, c * c, wtsv);
+    fa.tsv_nwgt = a.tsv_nwgt;
+    fa.kl_l = a.kl_l > 0 ? a.kl_l / Nz : a.kl_l;
+    fa.kl_wgt = scaled(a.kl_wgt, a.kl_nwgt, c, wkl);
+    fa.kl_nwgt = a.kl_nwgt;
+    fa.gs_l = a.gs_l > 0 ? a.gs_l / Nz : a.gs_l;
+    fa.gs_wgt = scaled(a.gs_wgt, a.gs_nwgt, c, wgs);
+    fa.gs_nwgt = a.gs_nwgt;
+    if (lc_on) {
+      fa.tfd_l = a.lc_l[z] > 0 ? a.lc_l[z] / Nz : a.lc_l[z];
+      fa.tfd_tgtfd = a.lc_tgtfd[z];
+    } else {
+      fa.tfd_l = a.tfd_l > 0 ? a.tfd_l / Nz : a.tfd_l;
+      fa.tfd_tgtfd = a.tfd_tgtfd;
+    }
+    fa.cen_l = -1.0;
+    fa.cen_alpha = 1.0;
+    fa.sm_l = a.sm_l > 0 ? a.sm_l / Nz : a.sm_l;
+    fa.sm_maj = a.sm_maj;
+    fa.sm_min = a.sm_min;
+    fa.sm_phi = a.sm_phi;
+    fa.isfcv = !f.ifcv.empty();
+    fa.nfcv = (int)f.ifcv.size();
+    fa.uvidxfcv = f.ifcv.data();
+    fa.vfcvr = f.fr.data();
+    fa.vfcvi = f.fi.data();
+    fa.varfcv = f.fv.data();
+    fa.wfcv = a.wfcv;
+    fa.isamp = !f.iamp.empty();
+    fa.namp = (int)f.iamp.size();
+    fa.uvidxamp = f.iamp.data();
+    fa.vamp = f.av.data();
+    fa.varamp = f.avar.data();
+    fa.wamp = a.wamp;
+    fa.iscp = !f.cpv.empty();
+    fa.ncp = (int)f.cpv.size();
+    fa.uvidxcp = f.icp.data();
+    fa.cp = f.cpv.data();
+    fa.varcp = f.cpvar.data();
+    fa.wcp = a.wcp;
+    fa.isca = !f.cav.empty();
+    fa.nca = (int)f.cav.size();
+    fa.uvidxca = f.ica.data();
+    fa.ca = f.cav.data();
+    fa.varca = f.cavar.data();
+    fa.wca = a.wca;
+    fa.inormfactr = a.inormfactr;
+    if ((rc = pack_problem<R>(fa, PK_FRAME, 0, nonneg, m, factr, pgtol, eps, ar, fh[z], nullptr, nullptr, nullptr,
+                              wtotal)) != SMILI_OK)
+      return rc;
+    ProbDesc& F = fh[z].d;
+    F.o_x = d.o_x + (int64_t)sizeof(double) * z * N;
+    F.o_g = d.o_g + (int64_t)sizeof(double) * z * N;
+    F.o_d = d.o_d + (int64_t)sizeof(double) * z * N;
+    F.nonneg = d.nonneg;
+  }
+  // blobs: movie vectors, then every frame's arrays and the frame descriptors
+  hp.put(d.o_x0, std::vector<double>(xsrc, xsrc + n));
+  hp.put(d.o_lcf, std::vector<double>(a.lc_tgtfd, a.lc_tgtfd + Nz));
+  if (d.has_rt) hp.put(d.o_rtw, std::vector<double>(a.rt_wgt, a.rt_wgt + N));
+  if (d.has_ri) hp.put(d.o_riw, std::vector<double>(a.ri_wgt, a.ri_wgt + N));
+  std::vector<ProbDesc> fdesc(Nz);
+  for (int z = 0; z < Nz; ++z) {
+    fdesc[z] = fh[z].d;
+    for (auto& bl : fh[z].blobs)
+      if (bl.first >= 0) hp.blobs.emplace_back(bl.first, std::move(bl.second));
+  }
+  hp.put(d.o_frames, fdesc);
+  return SMILI_OK;
+}
+
+template <typename R>
+int create_movie(const smili_imaging3d_args* a, int kind, int niter, int nonneg, int m, double factr,
+                 double pgtol, const smili_options* opt, const double* x_over, smili_batch** out) {
+  const double eps = (opt && opt->nufft_eps > 0) ? opt->nufft_eps : 1e-6;
+  if (!(eps < 1.0)) return fail(SMILI_ERR_ARG, "nufft_eps must be in (0, 1)");
+  if (m < 1 || m > SMILI_MAXM_DEV) return fail(SMILI_ERR_UNSUPPORTED, "L-BFGS-B memory m must be 1..6");
+  smili_batch* b = new smili_batch();
+  b->nprob = 1;
+  b->prec64 = sizeof(R) == 8;
+  b->device = opt ? opt->device : 0;
+  b->kind = kind;
+  Arena ar;
+  std::vector<HostProb> hps(1);
+  const int rc = pack_movie<R>(*a, kind, niter, nonneg, m, factr, pgtol, eps, ar, hps[0], x_over);
+  if (rc != SMILI_OK) {
+    delete b;
+    return rc;
+  }
+  b->descs.push_back(hps[0].d);
+  b->arena_bytes = ar.bytes;
+  return finish_batch<R>(b, hps, hps[0].d.npix, opt, out);
+}
+
+int create_movie_any(const smili_imaging3d_args* a, int kind, int niter, int nonneg, int m, double factr,
+                     double pgtol, const smili_options* opt, const double* x_over, smili_batch** out) {
+  if (!a || !out) return fail(SMILI_ERR_ARG, "null argument");
+  const int prec = opt && opt->precision ? opt->precision : 64;
+  if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
+  return prec == 64 ? create_movie<double>(a, kind, niter, nonneg, m, factr, pgtol, opt, x_over, out)
+                    : create_movie<float>(a, kind, niter, nonneg, m, factr, pgtol, opt, x_over, out);
+}
+
 int run(smili_batch* b, int mode, float* ms) {
   CUDA_TRY(cudaSetDevice(b->device));
   return b->prec64 ? launch_batch<double>(b, mode, ms) : launch_batch<float>(b, mode, ms);
@@ -975,7 +1459,7 @@ int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double
   if (grad) CUDA_TRY(cudaMemcpy(grad, b->d_arena + d.o_g, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
   ProbResult r;
   CUDA_TRY(cudaMemcpy(&r, b->d_results + p, sizeof(r), cudaMemcpyDeviceToHost));
-  if (terms) std::memcpy(terms, r.terms, sizeof(double) * SMILI_NTERMS);
+  if (terms) std::memcpy(terms, r.terms, sizeof(double) * (d.nframes > 0 ? SMILI_NTERMS3D : SMILI_NTERMS));
   if (info) {
     info->task = r.task;
     info->niter = r.iter;
@@ -1054,6 +1538,38 @@ int smili_calc_cost(const smili_imaging_args* a, const double* x, const smili_op
   if (rc != SMILI_OK) return rc;
   rc = run(b, MODE_FG, nullptr);
   if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
+  smili_batch_destroy(b);
+  return rc;
+}
+
+int smili_fftim3d_imaging(const smili_imaging3d_args* a, int niter, int nonneg, int nprint, int m, double factr,
+                          double pgtol, const smili_options* opt, double* iout, double* terms3d,
+                          smili_solve_info* info) {
+  (void)nprint;  // progress prints re-evaluate the cost at the same movie; no effect on the result
+  if (!a || !iout) return fail(SMILI_ERR_ARG, "null argument");
+  if (niter < 0) return fail(SMILI_ERR_ARG, "niter must be >= 0");
+  smili_batch* b = nullptr;
+  int rc = create_movie_any(a, PK_SOLVE, niter, nonneg, m, factr, pgtol, opt, nullptr, &b);
+  if (rc != SMILI_OK) return rc;
+  rc = run(b, MODE_SOLVE, nullptr);
+  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, iout, terms3d, nullptr, info);
+  smili_batch_destroy(b);
+  if (rc == SMILI_OK) {
+    const size_t n = (size_t)a->npix * a->nz;
+    for (size_t i = 0; i < n; ++i)
+      if (std::fabs(iout[i]) < 1e-10) iout[i] = 0.0;  // fftim3d.f90:466 (zeroeps)
+  }
+  return rc;
+}
+
+int smili_calc_cost3d(const smili_imaging3d_args* a, const double* x, const smili_options* opt, double* terms3d,
+                      double* grad) {
+  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+  smili_batch* b = nullptr;
+  int rc = create_movie_any(a, PK_FG, 0, 0, 5, 1e1, 0.0, opt, x, &b);
+  if (rc != SMILI_OK) return rc;
+  rc = run(b, MODE_FG, nullptr);
+  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms3d, grad, nullptr);
   smili_batch_destroy(b);
   return rc;
 }

@@ -6,3 +6,4 @@
 from . import image  # noqa: F401
 from . import fftim2d  # noqa: F401
 from . import fftlib  # noqa: F401
+from . import fftim3d  # noqa: F401

@@ -196,3 +196,23 @@ def test_target_stop(crescent32, lib):
     b.run()
     assert b.fetch(0)[3]["task"] == lib.TASK_STOP
     b.close()
+
+
+def test_survey_batch_mixed_sizes(lib):
+    """The survey configuration: problems of different image sizes (64..256),
+    visibility counts and regularizer weights in one launch give the same
+    solves as one launch per problem (FP64, 10 iterations)."""
+    from smili_b200 import synth
+    kws = [make_kw(synth.survey_problem(i, seed=3, niter=10, model=synth.nufft_model)) for i in range(8)]
+    assert len({int(k["nx"]) for k in kws}) >= 3
+    b = lib.Batch(kws, niter=10, options=lib.make_options(64, 1e-9))
+    b.run()
+    for p, kw in enumerate(kws):
+        s = lib.Batch([kw], niter=10, options=lib.make_options(64, 1e-9))
+        s.run()
+        _, ts, _, is_ = s.fetch(0)
+        s.close()
+        _, tb, _, ib = b.fetch(p)
+        assert ib["niter"] == is_["niter"]
+        assert abs(tb["cost"] - ts["cost"]) <= 1e-6 * abs(ts["cost"]), (p, tb["cost"], ts["cost"])
+    b.close()
