@@ -173,6 +173,16 @@ int smili_fftim3d_imaging(const smili_imaging3d_args* a, int niter, int nonneg, 
 int smili_calc_cost3d(const smili_imaging3d_args* a, const double* x, const smili_options* opt,
                       double* terms3d, double* grad);
 
+/* model_fcv / model_amp / model_cp / model_ca (src/fortlib/fftlib.f90:744-1254):
+ * exactly one data term of `a` is given (is* flags); regularizers are
+ * ignored.  chisq = sum over that term of resid^2 / var (2 (1 - cos resid)
+ * / var for closure phases), grad its gradient, and per datum the model and
+ * residual: complex for fcv (shifted back to the reference pixel as
+ * phashift_c2r does), real for amp / cp / ca (model_im, resid_im zero; cp
+ * wrapped into (-pi, pi]).  The output arrays may be NULL. */
+int smili_model_terms(const smili_imaging_args* a, const double* x, const smili_options* opt, double* chisq,
+                      double* grad, double* model_re, double* model_im, double* resid_re, double* resid_im);
+
 /* NUFFTs of the imaging path with the reference's conventions (sign "+",
  * modes -N/2..(N-1)/2 at pixels 1..N): fortlib.fftlib.nufft_fwd_real
  * (type 2, fftlib.f90:86-100) and nufft_adj_real1d (type 1, real part,

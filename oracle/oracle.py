@@ -352,3 +352,67 @@ def minimize(fun, x0, m=5, lower=None, nbd=None, factr=1e1, pgtol=0.0, maxiter=1
                 break
         task = opt.step(x, f, g)
     return x, np.array(trace), task
+
+
+def model_terms(kw: dict, term: str, x, eps=0.0):
+    """model_fcv / amp / cp / ca (fftlib.f90:744-1254) restated in numpy over
+    the oracle's transforms: (chisq, grad, model, resid) of one data term
+    with unit weight; model / resid complex for fcv, real otherwise."""
+    a = Args(kw)
+    k = a.keep
+    nx, ny = a.c.nx, a.c.ny
+    img = np.zeros((ny, nx))
+    img[k["yidx"] - 1, k["xidx"] - 1] = x
+    V = nufft2d2(k["u"], k["v"], img, eps)
+    rre, rim = np.zeros(V.size), np.zeros(V.size)
+    if term == "fcv":
+        idx, sg = np.abs(k["uvidxfcv"]) - 1, np.sign(k["uvidxfcv"])
+        dix, diy = a.c.nxref - nx / 2.0 - 1, a.c.nyref - ny / 2.0 - 1
+        ph = np.exp(1j * (k["u"][idx] * sg * dix + k["v"][idx] * sg * diy))
+        data = (k["vfcvr"] + 1j * k["vfcvi"]) * ph
+        model = np.where(sg > 0, V[idx], np.conj(V[idx]))
+        resid = data - model
+        var = k["varfcv"]
+        chisq = float(np.sum(np.abs(resid) ** 2 / var))
+        np.add.at(rre, idx, -2 / var * resid.real)
+        np.add.at(rim, idx, -2 / var * resid.imag * sg)
+        model, resid = model / ph, resid / ph
+    elif term == "amp":
+        idx = np.abs(k["uvidxamp"]) - 1
+        model = np.abs(V[idx])
+        resid = k["vamp"] - model
+        var = k["varamp"]
+        chisq = float(np.sum(resid ** 2 / var))
+        f = -2 * resid / var / model
+        np.add.at(rre, idx, f * V[idx].real)
+        np.add.at(rim, idx, f * V[idx].imag)
+    elif term == "cp":
+        ii = k["uvidxcp"].reshape(-1, 3)
+        idx, sg = np.abs(ii) - 1, np.sign(ii)
+        Vq = V[idx]
+        model = np.sum(np.angle(Vq) * sg, axis=1)
+        resid = k["cp"] - model
+        var = k["varcp"]
+        chisq = float(np.sum(2 * (1 - np.cos(resid)) / var))
+        f = -2 * np.sin(resid) / var
+        a2 = np.abs(Vq) ** 2
+        for q in range(3):
+            np.add.at(rre, idx[:, q], -f / a2[:, q] * Vq[:, q].imag * sg[:, q])
+            np.add.at(rim, idx[:, q], f / a2[:, q] * Vq[:, q].real * sg[:, q])
+        resid = np.arctan2(np.sin(resid), np.cos(resid))
+        model = np.arctan2(np.sin(model), np.cos(model))
+    else:
+        ii = k["uvidxca"].reshape(-1, 4)
+        idx = np.abs(ii) - 1
+        Vq = V[idx]
+        amp = np.abs(Vq)
+        model = np.log(amp[:, 0]) + np.log(amp[:, 1]) - np.log(amp[:, 2]) - np.log(amp[:, 3])
+        resid = k["ca"] - model
+        var = k["varca"]
+        chisq = float(np.sum(resid ** 2 / var))
+        f = -2 * resid / var
+        for q, s in enumerate((1, 1, -1, -1)):
+            np.add.at(rre, idx[:, q], s * f / amp[:, q] ** 2 * Vq[:, q].real)
+            np.add.at(rim, idx[:, q], s * f / amp[:, q] ** 2 * Vq[:, q].imag)
+    g2 = nufft2d1(k["u"], k["v"], rre - 1j * rim, nx, ny, eps).real
+    return chisq, g2[k["yidx"] - 1, k["xidx"] - 1], model, resid

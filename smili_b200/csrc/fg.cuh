@@ -240,6 +240,8 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
   const int e_amp = P.nfcv, e_cp = e_amp + P.namp, e_ca = e_cp + P.ncp, e_end = e_ca + P.nca;
   const int s_amp = P.nfcv, s_cp = s_amp + P.namp, s_ca = s_cp + 3 * P.ncp;
   const R wf = (R)P.wfcv, wa = (R)P.wamp, wc = (R)P.wcp, wq = (R)P.wca;
+  // model_fcv/amp/cp/ca (fftlib.f90:744-1254) also return each datum's model and residual
+  double* mres = P.o_model ? at<double>(c.base, P.o_model) : nullptr;
   for (int i = g.rank * SMILI_THREADS + threadIdx.x; i < e_end; i += g.G * SMILI_THREADS) {
     const R var = dvar[i];
     if (i < e_amp) {  // complex visibilities (fftlib.f90:384-439)
@@ -251,6 +253,12 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
       acc[0].add(((rr * rr + ri * ri) / var) * wf);
       const R factor = (R)-2 / var * wf;
       contrib[slot] = cmk(factor * rr, factor * ri * sg);
+      if (mres) {
+        mres[4 * i] = Vk.x;
+        mres[4 * i + 1] = sg * Vk.y;
+        mres[4 * i + 2] = rr;
+        mres[4 * i + 3] = ri;
+      }
     } else if (i < e_cp) {  // amplitudes (fftlib.f90:442-493)
       const int slot = s_amp + (i - e_amp);
       const cpx<R> Vk = V[didx[slot]];
@@ -259,6 +267,12 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
       acc[1].add((resid * resid / var) * wa);
       const R factor = (R)-2 * resid / var / model * wa;
       contrib[slot] = cmk(factor * Vk.x, factor * Vk.y);
+      if (mres) {
+        mres[4 * i] = model;
+        mres[4 * i + 1] = 0;
+        mres[4 * i + 2] = resid;
+        mres[4 * i + 3] = 0;
+      }
     } else if (i < e_ca) {  // closure phases (fftlib.f90:576-655)
       const int slot = s_cp + 3 * (i - e_cp);
       cpx<R> Vq[3];
@@ -287,6 +301,12 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
       const R factor = (R)-2 * sr / var * wc;
       for (int q = 0; q < 3; ++q)
         contrib[slot + q] = cmk(-factor / a2[q] * Vq[q].y * sg[q], factor / a2[q] * Vq[q].x * sg[q]);
+      if (mres) {  // unwrapped; the host wraps both into (-pi, pi] as model_cp does
+        mres[4 * i] = model;
+        mres[4 * i + 1] = 0;
+        mres[4 * i + 2] = resid;
+        mres[4 * i + 3] = 0;
+      }
     } else {  // log closure amplitudes (fftlib.f90:496-573)
       const int slot = s_ca + 4 * (i - e_ca);
       cpx<R> Vq[4];
@@ -302,6 +322,12 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
       for (int q = 0; q < 4; ++q) {
         const R f = (q < 2 ? factor : -factor) / (a[q] * a[q]);
         contrib[slot + q] = cmk(f * Vq[q].x, f * Vq[q].y);
+      }
+      if (mres) {
+        mres[4 * i] = model;
+        mres[4 * i + 1] = 0;
+        mres[4 * i + 2] = resid;
+        mres[4 * i + 3] = 0;
       }
     }
   }

@@ -72,6 +72,7 @@ struct ProbDesc {
   int64_t o_sbk, o_sbi, o_hist;         // bucketed breakpoints, bucket counts/cursors
   int64_t o_cand, o_lred, o_state;
   int64_t o_trace;                      // cost at each NEW_X (double[niter+2])
+  int64_t o_model;                      // per datum: model re, im, residual re, im (double), or 0
   int64_t o_frames;                     // movie: ProbDesc[nframes]
   int64_t o_rtw, o_riw, o_lcf, o_iavg;  // movie: Rt / Ri weights, light curve, pixel average
   int64_t o_out;                        // results: terms[15], counters

@@ -545,7 +545,8 @@ struct HostProb {
   }
 };
 
-enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4 };  // PK_FRAME: one frame of a movie
+// PK_FRAME: one frame of a movie; PK_MODEL: one evaluation that also returns per-datum models
+enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4, PK_MODEL = 5 };
 
 template <typename R>
 int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, int m, double factr,
@@ -597,7 +598,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.nyref = a.nyref;
   d.windowed = N != nx * ny;
   // data terms
-  const bool use_data = kind == PK_SOLVE || kind == PK_FG || frame;
+  const bool use_data = kind == PK_SOLVE || kind == PK_FG || kind == PK_MODEL || frame;
   const int nfcv = (use_data && a.isfcv) ? a.nfcv : 0;
   const int namp = (use_data && a.isamp) ? a.namp : 0;
   const int ncp = (use_data && a.iscp) ? a.ncp : 0;
@@ -622,7 +623,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.wcp = ncp ? a.wcp / wtotal : 0;
   d.wca = nca ? a.wca / wtotal : 0;
   // regularizers (active when lambda > 0, image.f90:112-175)
-  const bool use_reg = kind == PK_SOLVE || kind == PK_FG || frame;
+  const bool use_reg = kind == PK_SOLVE || kind == PK_FG || kind == PK_MODEL || frame;
   auto need_w = [&](double l, const double* wv, int nw, const char* nm) -> int {
     if (!(use_reg && l > 0)) return 0;
     if (!wv || nw != N) return fail(SMILI_ERR_ARG, std::string(nm) + " weights must have npix entries");
@@ -871,7 +872,8 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.o_x = ar.take(sizeof(double) * N);
     d.o_g = ar.take(sizeof(double) * N);
   }
-  if (kind == PK_SOLVE || kind == PK_FG) {
+  if (kind == PK_MODEL) d.o_model = ar.take(sizeof(double) * 4 * std::max(d.ndata, 1));
+  if (kind == PK_SOLVE || kind == PK_FG || kind == PK_MODEL) {
     d.o_z = ar.take(sizeof(double) * N);
     d.o_r = ar.take(sizeof(double) * N);
     d.o_d = ar.take(sizeof(double) * N);
@@ -1403,6 +1405,36 @@ int create_movie(const smili_imaging3d_args* a, int kind, int niter, int nonneg,
   return finish_batch<R>(b, hps, hps[0].d.npix, opt, out);
 }
 
+// One evaluation of a single data term with unit weight and no
+// regularizer: the raw chi-square sum and gradient of model_fcv / amp / cp /
+// ca (fftlib.f90:744-1254), with every datum's model and residual.
+template <typename R>
+int create_model(const smili_imaging_args& a, const double* x, const smili_options* opt, smili_batch** out) {
+  const double eps = (opt && opt->nufft_eps > 0) ? opt->nufft_eps : 1e-6;
+  if (!(eps < 1.0)) return fail(SMILI_ERR_ARG, "nufft_eps must be in (0, 1)");
+  const int nterm = (a.isfcv != 0) + (a.isamp != 0) + (a.iscp != 0) + (a.isca != 0);
+  if (nterm != 1) return fail(SMILI_ERR_ARG, "exactly one data term must be given");
+  const double w = a.isfcv ? a.wfcv : a.isamp ? a.wamp : a.iscp ? a.wcp : a.wca;
+  if (!(w > 0)) return fail(SMILI_ERR_ARG, "the data weight must be positive");
+  smili_imaging_args b0 = a;
+  b0.l1_l = b0.tv_l = b0.tsv_l = b0.kl_l = b0.gs_l = b0.tfd_l = b0.cen_l = b0.sm_l = -1.0;
+  smili_batch* b = new smili_batch();
+  b->nprob = 1;
+  b->prec64 = sizeof(R) == 8;
+  b->device = opt ? opt->device : 0;
+  b->kind = PK_MODEL;
+  Arena ar;
+  std::vector<HostProb> hps(1);
+  const int rc = pack_problem<R>(b0, PK_MODEL, 0, 0, 5, 1e1, 0.0, eps, ar, hps[0], x, nullptr, nullptr, w);
+  if (rc != SMILI_OK) {
+    delete b;
+    return rc;
+  }
+  b->descs.push_back(hps[0].d);
+  b->arena_bytes = ar.bytes;
+  return finish_batch<R>(b, hps, hps[0].d.npix, opt, out);
+}
+
 int create_movie_any(const smili_imaging3d_args* a, int kind, int niter, int nonneg, int m, double factr,
                      double pgtol, const smili_options* opt, const double* x_over, smili_batch** out) {
   if (!a || !out) return fail(SMILI_ERR_ARG, "null argument");
@@ -1570,6 +1602,48 @@ int smili_calc_cost3d(const smili_imaging3d_args* a, const double* x, const smil
   if (rc != SMILI_OK) return rc;
   rc = run(b, MODE_FG, nullptr);
   if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms3d, grad, nullptr);
+  smili_batch_destroy(b);
+  return rc;
+}
+
+int smili_model_terms(const smili_imaging_args* a, const double* x, const smili_options* opt, double* chisq,
+                      double* grad, double* model_re, double* model_im, double* resid_re, double* resid_im) {
+  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+  const int prec = opt && opt->precision ? opt->precision : 64;
+  if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
+  smili_batch* b = nullptr;
+  int rc = prec == 64 ? create_model<double>(*a, x, opt, &b) : create_model<float>(*a, x, opt, &b);
+  if (rc != SMILI_OK) return rc;
+  rc = run(b, MODE_FG, nullptr);
+  double terms[SMILI_NTERMS];
+  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
+  if (rc == SMILI_OK) {
+    const ProbDesc& d = b->descs[0];
+    std::vector<double> mr(4 * (size_t)d.ndata);
+    cudaError_t e = cudaMemcpy(mr.data(), b->d_arena + d.o_model, sizeof(double) * mr.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
+    } else {
+      if (chisq) *chisq = terms[0];
+      const double dix = a->nx / 2.0 + 1 - a->nxref, diy = a->ny / 2.0 + 1 - a->nyref;
+      for (int i = 0; i < d.ndata; ++i) {
+        std::complex<double> mo(mr[4 * i], mr[4 * i + 1]), re(mr[4 * i + 2], mr[4 * i + 3]);
+        if (a->isfcv) {  // phashift_c2r (fftlib.f90:200-220) of model and residual
+          const int k = std::abs(a->uvidxfcv[i]) - 1, sg = a->uvidxfcv[i] > 0 ? 1 : -1;
+          const std::complex<double> ph = std::exp(std::complex<double>(0.0, a->u[k] * sg * dix + a->v[k] * sg * diy));
+          mo *= ph;
+          re *= ph;
+        } else if (a->iscp) {  // model_cp wraps both into (-pi, pi] (fftlib.f90:1227-1228)
+          mo = std::atan2(std::sin(mo.real()), std::cos(mo.real()));
+          re = std::atan2(std::sin(re.real()), std::cos(re.real()));
+        }
+        if (model_re) model_re[i] = mo.real();
+        if (model_im) model_im[i] = mo.imag();
+        if (resid_re) resid_re[i] = re.real();
+        if (resid_im) resid_im[i] = re.imag();
+      }
+    }
+  }
   smili_batch_destroy(b);
   return rc;
 }
