@@ -198,6 +198,81 @@ def warm_start_cfg4(nprob, niter, rtol, device=0):
             "nrmse_truth_plain_fp64": nr(xs_p), "nrmse_truth_warm_fp32": nr(xs_w)}
 
 
+def dynamic_cfg5(niter, device=0, cpu_evals=2):
+    """Dynamic imaging (fftim3d): 64 frames of 128x128, ~6000 visibilities
+    per frame from 16 stations over 24 h, a crescent rotating by 90 deg,
+    complex visibilities + closure phases, l1 = tsv = 1 per frame, Rt = 1.
+    One movie solve (1000 iterations) in FP64 and FP32 on the device, and
+    the CPU restatement's time per evaluation (host threads) scaled to the
+    FP64 solve's evaluation count."""
+    from oracle import oracle as O
+    from smili_b200 import synth
+    from smili_b200.fortlib import fftim3d
+    from smili_b200.imaging.lbfgs3d import prepare_imaging3d
+    m = synth.dynamic_problem(seed=0, nframes=64, nx=128, nst=16, vis_per_frame=6000, niter=niter,
+                              model=synth.nufft_model)
+    kw, _ = prepare_imaging3d(m.frames, vistable=m.vistable, bstable=m.bstable, niter=niter, **m.reg)
+    out = {"frames": 64, "nx": 128, "visibilities": int(len(m.vistable)), "closure_phases": int(len(m.bstable)),
+           "parameters": int(np.size(kw["iin"])), "niter": niter}
+    for prec in (64, 32):
+        info = {}
+        t0 = time.perf_counter()
+        r = fftim3d.imaging(precision=prec, nufft_eps=1e-6, device=device, info=info, **kw)
+        dt = time.perf_counter() - t0
+        out[f"fp{prec}_solve_s"] = dt
+        out[f"fp{prec}_final_cost"] = r[20]
+        out[f"fp{prec}_nfg"] = info["nfg"]
+    O.build()
+    t0 = time.perf_counter()
+    for _ in range(cpu_evals):
+        O.calc_cost3d(kw, kw["iin"], eps=1e-6)
+    per = (time.perf_counter() - t0) / cpu_evals
+    out["cpu_port_s_per_eval"] = per
+    out["cpu_port_solve_s_scaled"] = per * out["fp64_nfg"]
+    out["cpu_cores"] = O.lib().orc_nthreads()
+    return out
+
+
+def large_cfg5(niter, device=0, cpu_evals=1):
+    """Large static image: 1024x1024 (1 uas pixels), 16 stations over 24 h
+    with ~5 s scans (~2e6 complex visibilities + closure phases), l1 = tsv
+    = 1, 50 uas Gaussian prior.  One FP64 and one FP32 solve on the device; the CPU restatement's
+    time per evaluation scaled to the FP64 evaluation count."""
+    from oracle import oracle as O
+    from smili_b200 import synth
+    from smili_b200.fortlib import fftim2d
+    from smili_b200.imaging.lbfgs import prepare_imaging
+    rng = np.random.default_rng(11)
+    img = synth.Image(1024, 1024, 1.0)
+    truth = synth.multigauss_gp_image(img, rng, ngauss=50, flux=1.0, extent_uas=200.0)
+    t = synth.observe(truth, img, rng, nst=16, dec_deg=12.0, freq_hz=230e9, hours=24.0, scan_min=5.2 / 60.0,
+                      fcv=True, cp=True, model=synth.nufft_model)
+    init = img.copy()
+    # a 50 uas prior: from 100-200 uas priors the first line search of the
+    # plain method (and of the CPU restatement) ends ABNORMAL at iteration 1
+    init.data[0, 0] = synth.gaussian_image(img, 50.0, 1.0)
+    kw, _ = prepare_imaging(init, vistable=t["vistable"], bstable=t["bstable"], niter=niter, l1_lambda=1.0,
+                            tsv_lambda=1.0)
+    out = {"nx": 1024, "visibilities": int(len(t["vistable"])), "closure_phases": int(len(t["bstable"])),
+           "niter": niter}
+    for prec in (64, 32):
+        info = {}
+        t0 = time.perf_counter()
+        r = fftim2d.imaging(precision=prec, nufft_eps=1e-6, device=device, info=info, **kw)
+        out[f"fp{prec}_solve_s"] = time.perf_counter() - t0
+        out[f"fp{prec}_final_cost"] = r[15]
+        out[f"fp{prec}_nfg"] = info["nfg"]
+    O.build()
+    t0 = time.perf_counter()
+    for _ in range(cpu_evals):
+        O.calc_cost(kw, kw["iin"], eps=1e-6)
+    per = (time.perf_counter() - t0) / cpu_evals
+    out["cpu_port_s_per_eval"] = per
+    out["cpu_port_solve_s_scaled"] = per * out["fp64_nfg"]
+    out["cpu_cores"] = O.lib().orc_nthreads()
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -236,6 +311,8 @@ def main():
     ap.add_argument("--target-rtol", type=float, default=1e-4)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--config5", action="store_true",
+                    help="also solve the 64-frame movie and the 1024x1024 / 2e6-visibility image")
     ap.add_argument("--warm-problems", type=int, default=64,
                     help="held-out problems of the learned warm-start comparison (0: skip)")
     args = ap.parse_args()
@@ -411,6 +488,9 @@ def main():
             "clocks": clk.summary(),
             "stage_ms_problem0": {k: round(v, 3) for k, v in stages.items()},
         }
+        if args.config5:
+            line["dynamic_cfg5"] = dynamic_cfg5(args.niter, local)
+            line["large_cfg5"] = large_cfg5(args.niter, local)
         if args.warm_problems > 0:
             line["warm_start_cfg4"] = warm_start_cfg4(args.warm_problems, args.niter, args.target_rtol, local)
         if not args.no_cpu:

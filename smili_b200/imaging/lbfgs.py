@@ -298,3 +298,138 @@ def imaging(initimage, **kwargs):
     kw, meta = prep
     output = fortlib.fftim2d.imaging(**kw)
     return finish_imaging(initimage, output, meta)
+
+
+# ---------------------------------------------------------------------------
+# statistics (lbfgs.py:578-755) and the chi-squares behind it
+# ---------------------------------------------------------------------------
+def _image_grid(image, mask, istokes, ifreq):
+    """Pixel vector, 1-based pixel indices, phase centre and uv scaling of an
+    image, windowed by ``mask`` (vistable.py:435-495)."""
+    Iin = np.float64(image.data[istokes, ifreq])
+    Nx, Ny = int(image.header["nx"]), int(image.header["ny"])
+    xidx, yidx = np.meshgrid(np.arange(Nx) + 1, np.arange(Ny) + 1)
+    if mask is None:
+        Iin, xidx, yidx = Iin.reshape(-1), xidx.reshape(-1), yidx.reshape(-1)
+    else:
+        idx = np.where(mask)
+        Iin, xidx, yidx = Iin[idx], xidx[idx], yidx[idx]
+    return (Iin, np.int32(xidx), np.int32(yidx), float(image.header["nxref"]), float(image.header["nyref"]),
+            Nx, Ny, np.deg2rad(image.header["dx"]), np.deg2rad(image.header["dy"]))
+
+
+def chisq_image(table, kind, image, mask=None, istokes=0, ifreq=0, **opt):
+    """``chisq_image`` of a VisTable (kind "fcv" or "amp"), BSTable ("cp")
+    or CATable ("ca") for an image (vistable.py:416-433, bstable.py:300-330,
+    catable.py:260-290): (chisq, reduced chisq) from model_fcv / amp / cp /
+    ca on the GPU, with the table's own values (no intensity normalisation)."""
+    Iin, xidx, yidx, nxref, nyref, Nx, Ny, dx, dy = _image_grid(image, mask, istokes, ifreq)
+    args = dict(fcvtable=None, amptable=None, bstable=None, catable=None)
+    args[{"fcv": "fcvtable", "amp": "amptable", "cp": "bstable", "ca": "catable"}[kind]] = table
+    u, v, ifcv, iamp, icp, ica = tools.get_uvlist(**args)
+    u = u * (2 * np.pi * dx)
+    v = v * (2 * np.pi * dy)
+    base = (Iin, xidx, yidx, nxref, nyref, Nx, Ny, u, v)
+    if kind == "fcv":
+        ph = np.deg2rad(np.asarray(table["phase"], dtype=np.float64))
+        amp = np.asarray(table["amp"], dtype=np.float64)
+        out = fortlib.fftlib.model_fcv(*base, ifcv, amp * np.cos(ph), amp * np.sin(ph),
+                                       np.square(np.asarray(table["sigma"], dtype=np.float64)), **opt)
+        n = 2 * len(table)
+    elif kind == "amp":
+        out = fortlib.fftlib.model_amp(*base, iamp, np.asarray(table["amp"], dtype=np.float64),
+                                       np.square(np.asarray(table["sigma"], dtype=np.float64)), **opt)
+        n = len(table)
+    elif kind == "cp":
+        out = fortlib.fftlib.model_cp(*base, icp, np.deg2rad(np.asarray(table["phase"], dtype=np.float64)),
+                                      np.square(np.asarray(table["sigma"], dtype=np.float64)
+                                                / np.asarray(table["amp"], dtype=np.float64)), **opt)
+        n = len(table)
+    else:
+        out = fortlib.fftlib.model_ca(*base, ica, np.asarray(table["logamp"], dtype=np.float64),
+                                      np.square(np.asarray(table["logsigma"], dtype=np.float64)), **opt)
+        n = len(table)
+    return out[0], out[0] / n
+
+
+def image_costs(image, istokes=0, ifreq=0):
+    """(l1, tv, tsv) of an image: the per-pixel functions l1_e, tv_e and
+    tsv_e of image.f90:245-257, 477-520, 678-720 summed over all pixels.
+    (The reference's ``imagecost`` calls fortlib.image.i2d_l1 / i2d_tv /
+    i2d_tsv, which its Fortran sources do not define; these sums are what
+    their names and the per-pixel functions describe.)"""
+    I = np.float64(image.data[istokes, ifreq])
+    l1 = float(np.sum(np.sqrt(I * I + 1e-10)))
+    dIx = np.zeros_like(I)
+    dIy = np.zeros_like(I)
+    dIx[:, :-1] = I[:, 1:] - I[:, :-1]
+    dIy[:-1, :] = I[1:, :] - I[:-1, :]
+    return l1, float(np.sum(np.sqrt(dIx * dIx + dIy * dIy))), float(np.sum(dIx * dIx + dIy * dIy))
+
+
+def statistics(initimage, imregion=None, vistable=None, amptable=None, bstable=None, catable=None,
+               lambl1=-1., lambtv=-1., lambtsv=-1., lambmem=-1., lambcom=-1., normlambda=True,
+               reweight=False, dyrange=1e6, niter=1000, nonneg=True, compower=1., totalflux=None,
+               fluxconst=False, istokes=0, ifreq=0, **opt):
+    """Chi-squares and regularization costs of an image (lbfgs.py:578-755):
+    the same OrderedDict of keys.  ``opt`` passes precision / nufft_eps /
+    device to the GPU evaluations."""
+    import collections
+    if vistable is None and amptable is None and bstable is None and catable is None:
+        print("Error: No data are input.")
+        return -1
+    imagewin = imregion.imagewin(initimage, istokes, ifreq) if imregion is not None else None
+    if totalflux is None:
+        tf = []
+        if vistable is not None:
+            tf.append(np.asarray(vistable["amp"]).max())
+        if amptable is not None:
+            tf.append(np.asarray(amptable["amp"]).max())
+        totalflux = np.max(tf)
+    Ndata = 0
+    res = {}
+    for key, table, kind, nd in (("fcv", vistable, "fcv", 2), ("amp", amptable, "amp", 1),
+                                 ("cp", bstable, "cp", 1), ("ca", catable, "ca", 1)):
+        if table is None:
+            res[key] = (False, 0., 0.)
+        else:
+            c, rc = chisq_image(table, kind, initimage, imagewin, istokes, ifreq, **opt)
+            res[key] = (True, c, rc)
+            Ndata += len(table) * nd
+    Nx, Ny = int(initimage.header["nx"]), int(initimage.header["ny"])
+    Nyx = Nx * Ny
+    if normlambda:
+        fluxscale = np.abs(np.float64(totalflux)) / Nyx
+        lambl1_sim = lambl1 / (fluxscale * Nyx)
+        lambtv_sim = lambtv / (4 * fluxscale * Nyx)
+        lambtsv_sim = lambtsv / (4 * fluxscale ** 2 * Nyx)
+    else:
+        lambl1_sim, lambtv_sim, lambtsv_sim = lambl1, lambtv, lambtsv
+    l1, tv, tsv = image_costs(initimage, istokes, ifreq)
+    if lambl1 > 0:
+        l1cost = l1 * lambl1_sim
+    else:
+        lambl1 = lambl1_sim = l1cost = 0.
+    if lambtv > 0:
+        tvcost = tv * lambtv_sim
+    else:
+        lambtv = lambtv_sim = tvcost = 0.
+    if lambtsv > 0:
+        tsvcost = tsv * lambtsv_sim
+    else:
+        lambtsv = lambtsv_sim = tsvcost = 0.
+    stats = collections.OrderedDict()
+    stats["cost"] = l1cost + tvcost + tsvcost
+    stats["chisq"] = res["fcv"][1] + res["amp"][1] + res["cp"][1] + res["ca"][1]
+    stats["rchisq"] = stats["chisq"] / Ndata
+    stats["cost"] += stats["rchisq"]
+    for key in ("fcv", "amp", "cp", "ca"):
+        stats["is" + key] = res[key][0]
+    for key in ("fcv", "amp", "cp", "ca"):
+        stats["chisq" + key] = res[key][1]
+    for key in ("fcv", "amp", "cp", "ca"):
+        stats["rchisq" + key] = res[key][2]
+    stats["lambl1"], stats["lambl1_sim"], stats["l1"], stats["l1cost"] = lambl1, lambl1_sim, l1, l1cost
+    stats["lambtv"], stats["lambtv_sim"], stats["tv"], stats["tvcost"] = lambtv, lambtv_sim, tv, tvcost
+    stats["lambtsv"], stats["lambtsv_sim"], stats["tsv"], stats["tsvcost"] = lambtsv, lambtsv_sim, tsv, tsvcost
+    return stats

@@ -65,3 +65,23 @@ def test_model_terms_reject_two_terms(crescent32):
     x = np.ascontiguousarray(kw["iin"], dtype=np.float64)
     rc = lib.lib().smili_model_terms(C.addressof(prob.c), lib.dptr(x), None, None, None, None, None, None, None)
     assert rc == -1
+
+
+def test_statistics_uses_model_terms(oracle, crescent32):
+    """statistics(): chi-squares of the tables from the model terms and the
+    image costs; against the oracle's model terms and numpy sums."""
+    from smili_b200.imaging.lbfgs import statistics
+    o = crescent32
+    st = statistics(o.image, vistable=o.vistable, bstable=o.bstable, lambl1=1.0, lambtsv=1.0, nufft_eps=1e-12)
+    kw = make_kw(o)
+    x = np.asarray(kw["iin"]) / float(kw["inormfactr"])
+    # the oracle on the raw (unnormalised) data of the same tables
+    raw = dict(kw, vfcvr=kw["vfcvr"] / kw["inormfactr"], vfcvi=kw["vfcvi"] / kw["inormfactr"],
+               varfcv=kw["varfcv"] / kw["inormfactr"] ** 2)
+    cf = oracle.model_terms(raw, "fcv", x, eps=0.0)[0]
+    cc = oracle.model_terms(raw, "cp", x, eps=0.0)[0]
+    assert abs(st["chisqfcv"] - cf) <= 1e-9 * cf and abs(st["chisqcp"] - cc) <= 1e-9 * cc
+    assert abs(st["rchisq"] - (cf + cc) / (2 * len(o.vistable) + len(o.bstable))) <= 1e-9 * st["rchisq"]
+    I = o.image.data[0, 0]
+    assert abs(st["l1"] - np.sum(np.sqrt(I * I + 1e-10))) <= 1e-12 * st["l1"]
+    assert st["isfcv"] and st["iscp"] and not st["isamp"] and not st["isca"]
