@@ -73,9 +73,10 @@ def dirty_images(kws, device=0, chunk=1024):
     return np.asarray(out, np.float32)
 
 
-def solve(kws, niter, precision=64, targets=None, device=0, x0=None, chunk=1024):
+def solve(kws, niter, precision=64, targets=None, device=0, x0=None, chunk=1024, ctas_per_problem=0):
     """Batched L-BFGS-B solves (``chunk`` problems per launch); x0 (list of
-    pixel vectors in scaled units) replaces the kwargs' initial images.
+    pixel vectors in scaled units) replaces the kwargs' initial images;
+    ``ctas_per_problem`` fixes the CTA group size (0: automatic).
     Returns (x list, info list, cost array, traces, total kernel ms)."""
     xs, infos, costs, traces, ms = [], [], [], [], 0.0
     for c0 in range(0, len(kws), chunk):
@@ -85,7 +86,8 @@ def solve(kws, niter, precision=64, targets=None, device=0, x0=None, chunk=1024)
             if x0 is not None:
                 k["iin"] = x0[i]
             probs.append(k)
-        b = _lib.Batch(probs, niter=niter, options=_lib.make_options(precision, 1e-6, device=device))
+        b = _lib.Batch(probs, niter=niter, options=_lib.make_options(precision, 1e-6, ctas_per_problem,
+                                                                     device=device))
         if targets is not None:
             b.set_targets(np.asarray(targets)[c0:c0 + len(probs)])
         ms += b.run()
