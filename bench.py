@@ -21,7 +21,9 @@ more, in one batch).  ``value`` counts every solve; ``value_strict`` only
 those that reached their plain solve's final cost.
 
 One step = one batched FP32 solve of ``--batch`` problems (device-resident
-inputs, persistent launch).  ``value`` = solves per second over the timed
+inputs, persistent launch, launch shape chosen by ``smili_b200.autotune``;
+296 problems on 148 resident CTA groups, so a group that finishes early
+takes a queued problem).  ``value`` = solves per second over the timed
 steps; ``e2e`` = the same metric through the C
 ABI from host buffers (upload, solve, download of every image inside the
 timed region); ``plain_fp64`` reports single-problem FP64 solves/s;
@@ -313,7 +315,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=148)
+    ap.add_argument("--batch", type=int, default=296)
     ap.add_argument("--seeds", type=int, default=16)
     ap.add_argument("--niter", type=int, default=1000)
     ap.add_argument("--ref-iters", type=int, default=60)
@@ -396,9 +398,14 @@ def main():
     control = quality(ctl, S, np.arange(S))
     ctl.close()
 
+    # launch shape (CTAs per problem, spreading tile) from the autotuner,
+    # timed on short solves of this batch
+    from smili_b200 import autotune
+    tuned = autotune.tune(probs, 32, niter=20, repeats=2, device=local,
+                          cands=[(2, 8), (3, 8), (4, 8), (3, 16)])
     # FP32 batched, inputs resident on the device: the reference's iteration
     # budget with an early exit at the plain solve's final cost
-    opts = _lib.make_options(32, 1e-6, device=local)
+    opts = _lib.make_options(32, 1e-6, tuned["ctas_per_problem"], local, spread_bin=tuned["spread_bin"])
     ftarget = targets[seed_of]
     batch = _lib.Batch(probs, niter=args.niter, options=opts)
     batch.set_targets(ftarget)
@@ -472,6 +479,8 @@ def main():
                                    f"L-BFGS-B m=5, {args.niter} iterations with an early exit at the "
                                    f"plain FP64 solve's final cost x (1 + {args.target_rtol:g})",
                        "batch": B, "distinct_seeds": S,
+                       "launch": {"ctas_per_problem": tuned["ctas_per_problem"],
+                                  "spread_bin": tuned["spread_bin"], "chosen_by": "autotuner (20-iteration solves)"},
                        "precision": "FP32 transforms + compensated chi-square, FP64 L-BFGS-B",
                        "warm_start": "not applicable to this workload: its station-based gains "
                                      "scramble visibility phases, so no dirty image exists to start "

@@ -68,6 +68,9 @@ typedef struct {
   int ctas_per_problem; /* 0 -> automatic */
   int device;           /* CUDA device ordinal */
   void* stream;         /* cudaStream_t, NULL -> the library's own stream */
+  int spread_bin;       /* spreading tile side in fine-grid cells: 8 or 16; 0 -> 8.  A
+                           16-cell tile whose subgrids do not fit in shared memory
+                           falls back to 8 */
 } smili_options;
 
 typedef struct {

@@ -354,7 +354,6 @@ __device__ __forceinline__ R warp_sum(R v) {
 // points are ordered by __syncwarp), so the inner loop needs no atomics.  The
 // finished subgrid is added to the CTA's band copy (shared atomics, only the
 // overlapping halos collide) and the CTA's band to the global band at the end.
-#define SMILI_BIN 8
 template <typename R>
 __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
   const ProbDesc& P = *c.P;
@@ -366,7 +365,7 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
   const cpx<R>* contrib = at<cpx<R>>(c.base, P.o_contrib);
   R* gband = at<R>(c.base, P.o_bandC);
   const int w = P.w, ww = P.w * P.w;
-  const int SG = SMILI_BIN + w - 1;  // subgrid side
+  const int SG = P.bin + w - 1;  // subgrid side
   const R beta = (R)P.beta;
   const R half = (R)0.5 * (R)w, inv = (R)1 / half;
   const int ncell = P.b1n * P.b2n;

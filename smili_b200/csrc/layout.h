@@ -40,7 +40,8 @@ struct ProbDesc {
   int nonneg, m, niter, prec64;
   int has_l1, has_tv, has_tsv, has_kl, has_gs, has_tfd, has_cen, has_sm;
   int windowed;            // 1 when the pixel set is not the full nx*ny grid
-  int nitems;              // spreading work items (<= 128 points of one 8x8 bin)
+  int nitems;              // spreading work items (<= 128 points of one bin x bin tile)
+  int bin;                 // spreading bin side in fine-grid cells (8 or 16)
   // movies (dynamic imaging): nframes >= 1 on a movie's descriptor (0 for a
   // 2D problem), whose vectors hold npix = frame_npix * nframes values; each
   // frame is a 2D descriptor (o_frames) whose x / g / d point into them

@@ -551,7 +551,7 @@ enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4, PK_MODEL = 5
 template <typename R>
 int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, int m, double factr,
                  double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override,
-                 const double* c_re, const double* c_im, double wtotal_override = 0.0) {
+                 const double* c_re, const double* c_im, double wtotal_override = 0.0, int bin = 8) {
   ProbDesc& d = hp.d;
   std::memset(&d, 0, sizeof(d));
   const int N = a.npix, nx = a.nx, ny = a.ny, nuv = a.nuv;
@@ -707,8 +707,18 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.b2s = (int)mn2;
     d.b2n = (int)(mx2 - mn2 + 1);
   }
-  // sort the uv points by 8x8 bins of the band (spreading subproblems and
-  // locality); remap indices.  Band-relative cells are computed exactly as the
+  // spreading tile: 16 x 16 when its warp subgrids (8 warps of (16 + w - 1)^2
+  // complex values) and the smallest weight table fit the dynamic shared
+  // memory of the launch, else 8 x 8
+  {
+    const size_t dyn = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
+    const size_t sg = 16 + w - 1;
+    if (bin == 16 && 8 * sg * sg * sizeof(cpx<R>) + 8 * 8 * 2 * w * sizeof(R) + 16 > dyn) bin = 8;
+    if (bin != 16) bin = 8;
+  }
+  d.bin = bin;
+  // sort the uv points by bin x bin tiles of the band (spreading subproblems
+  // and locality); remap indices.  Band-relative cells are computed exactly as the
   // kernels do: imod(ceil(xi - w/2) - start, nf).
   auto imodh = [](long a, long n) {
     long r = a % n;
@@ -720,7 +730,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   for (int j = 0; j < nuv; ++j) {
     const long c1 = imodh((long)std::ceil(xu[j] - half) - d.b1s, d.nf1);
     const long c2 = imodh((long)std::ceil(xv[j] - half) - d.b2s, d.nf2);
-    bkey[j] = ((c2 >> 3) << 32) + (c1 >> 3);
+    bkey[j] = ((c2 / bin) << 32) + (c1 / bin);
   }
   std::stable_sort(perm.begin(), perm.end(), [&](int p, int q) { return bkey[p] < bkey[q]; });
   // spreading work items: <= 128 consecutive points of one bin
@@ -731,8 +741,8 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     while (e < nuv && bkey[perm[e]] == k && e - j < 128) ++e;
     items.push_back(j);
     items.push_back(e);
-    items.push_back((int)((k >> 32) * 8));
-    items.push_back((int)((k & 0xffffffffL) * 8));
+    items.push_back((int)((k >> 32) * bin));
+    items.push_back((int)((k & 0xffffffffL) * bin));
     j = e;
   }
   d.nitems = (int)items.size() / 4;
@@ -1018,7 +1028,8 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   int maxn = 1;
   for (int p = 0; p < nprob; ++p) {
     const int rc = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ar,
-                                   hps[p], x_over ? x_over[p] : nullptr, c_re, c_im);
+                                   hps[p], x_over ? x_over[p] : nullptr, c_re, c_im, 0.0,
+                                   opt && opt->spread_bin ? opt->spread_bin : 8);
     if (rc != SMILI_OK) {
       delete b;
       return rc;
@@ -1134,7 +1145,7 @@ int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smi
 // movie's vectors.
 template <typename R>
 int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, int m, double factr,
-               double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override) {
+               double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override, int spread_bin) {
   const int N = a.npix, Nz = a.nz, nuv = a.nuv;
   if (N < 1 || Nz < 1 || nuv < 0 || a.nx < 1 || a.ny < 1 || (long)N * Nz > 0x7fffffffL)
     return fail(SMILI_ERR_ARG, "invalid movie sizes");
@@ -1359,7 +1370,7 @@ int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, i
     fa.wca = a.wca;
     fa.inormfactr = a.inormfactr;
     if ((rc = pack_problem<R>(fa, PK_FRAME, 0, nonneg, m, factr, pgtol, eps, ar, fh[z], nullptr, nullptr, nullptr,
-                              wtotal)) != SMILI_OK)
+                              wtotal, spread_bin)) != SMILI_OK)
       return rc;
     ProbDesc& F = fh[z].d;
     F.o_x = d.o_x + (int64_t)sizeof(double) * z * N;
@@ -1395,7 +1406,8 @@ int create_movie(const smili_imaging3d_args* a, int kind, int niter, int nonneg,
   b->kind = kind;
   Arena ar;
   std::vector<HostProb> hps(1);
-  const int rc = pack_movie<R>(*a, kind, niter, nonneg, m, factr, pgtol, eps, ar, hps[0], x_over);
+  const int rc = pack_movie<R>(*a, kind, niter, nonneg, m, factr, pgtol, eps, ar, hps[0], x_over,
+                               opt && opt->spread_bin ? opt->spread_bin : 8);
   if (rc != SMILI_OK) {
     delete b;
     return rc;
@@ -1425,7 +1437,8 @@ int create_model(const smili_imaging_args& a, const double* x, const smili_optio
   b->kind = PK_MODEL;
   Arena ar;
   std::vector<HostProb> hps(1);
-  const int rc = pack_problem<R>(b0, PK_MODEL, 0, 0, 5, 1e1, 0.0, eps, ar, hps[0], x, nullptr, nullptr, w);
+  const int rc = pack_problem<R>(b0, PK_MODEL, 0, 0, 5, 1e1, 0.0, eps, ar, hps[0], x, nullptr, nullptr, w,
+                                 opt && opt->spread_bin ? opt->spread_bin : 8);
   if (rc != SMILI_OK) {
     delete b;
     return rc;

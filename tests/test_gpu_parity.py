@@ -216,3 +216,26 @@ def test_survey_batch_mixed_sizes(lib):
         assert ib["niter"] == is_["niter"]
         assert abs(tb["cost"] - ts["cost"]) <= 1e-6 * abs(ts["cost"]), (p, tb["cost"], ts["cost"])
     b.close()
+
+
+def test_spread_bin16_equals_bin8(oracle, closure40, lib):
+    """16-cell spreading tiles give the same evaluation as 8-cell tiles (and
+    as the oracle); the autotuner returns one of its candidates."""
+    from smili_b200 import autotune
+    from smili_b200.fortlib import fftim2d
+    kw = make_kw(closure40)
+    x = np.asarray(kw["iin"]) * np.random.default_rng(2).uniform(0.5, 1.5, np.size(kw["iin"]))
+    prob = lib.Problem(dict(kw, iin=x))
+    out = []
+    for b in (8, 16):
+        bt = lib.Batch([prob], niter=1, options=lib.make_options(64, 1e-12, spread_bin=b))
+        bt.run(fg_only=1)
+        _, t, g, _ = bt.fetch(0)
+        bt.close()
+        out.append((t["cost"], g))
+    assert abs(out[1][0] - out[0][0]) <= 1e-12 * abs(out[0][0])
+    assert np.max(np.abs(out[1][1] - out[0][1])) <= 1e-10 * np.max(np.abs(out[0][1]))
+    t_o, g_o = oracle.calc_cost(kw, x, eps=0.0)
+    assert abs(out[1][0] - t_o["cost"]) <= 1e-9 * abs(t_o["cost"])
+    r = autotune.tune([kw] * 4, 32, niter=3, repeats=1, cands=[(1, 8), (2, 16)])
+    assert (r["ctas_per_problem"], r["spread_bin"]) in [(1, 8), (2, 16)] and len(r["table"]) == 2
