@@ -21,9 +21,7 @@ more, in one batch).  ``value`` counts every solve; ``value_strict`` only
 those that reached their plain solve's final cost.
 
 One step = one batched FP32 solve of ``--batch`` problems (device-resident
-inputs, persistent launch, launch shape chosen by ``smili_b200.autotune``;
-296 problems on 148 resident CTA groups, so a group that finishes early
-takes a queued problem).  ``value`` = solves per second over the timed
+inputs, persistent launch, launch shape chosen by ``smili_b200.autotune``).  ``value`` = solves per second over the timed
 steps; ``e2e`` = the same metric through the C
 ABI from host buffers (upload, solve, download of every image inside the
 timed region); ``plain_fp64`` reports single-problem FP64 solves/s;
@@ -315,7 +313,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=296)
+    ap.add_argument("--batch", type=int, default=148)
     ap.add_argument("--seeds", type=int, default=16)
     ap.add_argument("--niter", type=int, default=1000)
     ap.add_argument("--ref-iters", type=int, default=60)

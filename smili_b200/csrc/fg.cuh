@@ -24,6 +24,14 @@ __device__ __forceinline__ R es_kernel(R z, R beta) {
   return s > (R)0 ? exp(beta * (sqrt(s) - (R)1)) : (R)0;
 }
 
+// FP32: the hardware exponential; its error (a few ulps over the kernel's
+// argument range [-beta, 0]) is far below the 1e-6 tolerance of the transform
+template <>
+__device__ __forceinline__ float es_kernel<float>(float z, float beta) {
+  const float s = 1.f - z * z;
+  return s > 0.f ? __expf(beta * (sqrtf(s) - 1.f)) : 0.f;
+}
+
 __device__ __forceinline__ int imod(int a, int n) {
   if ((unsigned)a < (unsigned)n) return a;  // the common case
   int r = a % n;
@@ -354,8 +362,167 @@ __device__ __forceinline__ R warp_sum(R v) {
 // points are ordered by __syncwarp), so the inner loop needs no atomics.  The
 // finished subgrid is added to the CTA's band copy (shared atomics, only the
 // overlapping halos collide) and the CTA's band to the global band at the end.
+// ---------------------------------------------------------------------------
+// F5 on the tensor cores (FP32, w <= 9, 8 x 8 tiles).  A tile's subgrid is a
+// product of two thin matrices:
+//   D[r][c] = sum_p wy_p[r] (c_p wx_p[c]),   r, c < 8 + w - 1 <= 16,
+// with wy_p / wx_p the point's kernel weights placed at its offset inside
+// the subgrid (zero elsewhere) and c_p = Vres_re - i Vres_im of the point.
+// A warp accumulates the real and imaginary parts of one tile's 16 x 16
+// subgrid in mma.sync.m16n8k8 TF32 fragments (8 points per k step) with the
+// three-term split a b ~ ah bh + ah bl + al bh (a = ah + al in TF32), which
+// keeps the products within a few FP32 ulps; the subgrid never touches
+// shared memory and no tap waits on another.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ void fg_spread_tc(FgCtx<float>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const float* xu = at<float>(c.base, P.o_u);
+  const float* xv = at<float>(c.base, P.o_v);
+  const int* off = at<int>(c.base, P.o_csr_off);
+  const int* ent = at<int>(c.base, P.o_csr_ent);
+  const int4* items = at<int4>(c.base, P.o_items);
+  const cpx<float>* contrib = at<cpx<float>>(c.base, P.o_contrib);
+  float* gband = at<float>(c.base, P.o_bandC);
+  const int w = P.w;
+  const int SG = 8 + w - 1;  // <= 16
+  const float beta = (float)P.beta;
+  const float half = 0.5f * (float)w, inv = 1.f / half;
+  const int ncell = P.b1n * P.b2n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int gq = lane >> 2, t = lane & 3;
+  // shared memory: [nw][32 points][2w] kernel weights, then (if it fits) a
+  // private copy of the band
+  const size_t wt_b = ((size_t)nw * 32 * 2 * w * sizeof(float) + 15) / 16 * 16;
+  float* wtab = reinterpret_cast<float*>(c.sbuf) + (size_t)warp * 32 * 2 * w;
+  cpx<float>* sband = reinterpret_cast<cpx<float>*>(reinterpret_cast<char*>(c.sbuf) + wt_b);
+  const bool staged = wt_b + (size_t)ncell * sizeof(cpx<float>) <= (size_t)c.dyn_cpx * sizeof(cpx<float>);
+  float* band = staged ? reinterpret_cast<float*>(sband) : gband;
+  if (staged) {
+    for (int i = threadIdx.x; i < ncell; i += blockDim.x) sband[i] = cmk<float>(0, 0);
+    __syncthreads();
+  }
+  const int gw = g.rank * nw + warp, nwt = g.G * nw;
+  for (int it = gw; it < P.nitems; it += nwt) {
+    const int4 item = items[it];
+    float dre[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}}, dim[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+    for (int jb = item.x; jb < item.y; jb += 32) {
+      // phase 1: every lane prepares one point (zero weights past the item)
+      const int jl = jb + lane;
+      float cre_l = 0.f, cim_l = 0.f;
+      int lr_l = 0, lc_l = 0;
+      float* wr = wtab + lane * 2 * w;
+      if (jl < item.y) {
+        const int e1 = off[jl + 1];
+        for (int e = off[jl]; e < e1; ++e) {
+          const cpx<float> q = contrib[ent[e]];
+          cre_l += q.x;
+          cim_l += q.y;
+        }
+        cim_l = -cim_l;  // c = Vresre - i Vresim
+        const float xi1 = xu[jl], xi2 = xv[jl];
+        const int l1 = (int)ceilf(xi1 - half), l2 = (int)ceilf(xi2 - half);
+        for (int q = 0; q < w; ++q) {
+          wr[q] = es_kernel(((float)(l1 + q) - xi1) * inv, beta);
+          wr[w + q] = es_kernel(((float)(l2 + q) - xi2) * inv, beta);
+        }
+        lr_l = imod(l2 - P.b2s, P.nf2) - item.z;
+        lc_l = imod(l1 - P.b1s, P.nf1) - item.w;
+      } else {
+        for (int q = 0; q < 2 * w; ++q) wr[q] = 0.f;
+      }
+      __syncwarp();
+      // phase 2: 8 points per k step; lane (gq, t) feeds points t and t + 4
+      const int np = min(32, item.y - jb);
+      for (int kb = 0; kb < np; kb += 8) {
+        const int p0 = kb + t, p1 = kb + t + 4;
+        const int lr0 = __shfl_sync(0xffffffffu, lr_l, p0), lr1 = __shfl_sync(0xffffffffu, lr_l, p1);
+        const int lc0 = __shfl_sync(0xffffffffu, lc_l, p0), lc1 = __shfl_sync(0xffffffffu, lc_l, p1);
+        const float cr0 = __shfl_sync(0xffffffffu, cre_l, p0), cr1 = __shfl_sync(0xffffffffu, cre_l, p1);
+        const float ci0 = __shfl_sync(0xffffffffu, cim_l, p0), ci1 = __shfl_sync(0xffffffffu, cim_l, p1);
+        const float* w0 = wtab + p0 * 2 * w;
+        const float* w1 = wtab + p1 * 2 * w;
+        auto wy = [&](const float* wp, int d) { return (unsigned)d < (unsigned)w ? wp[w + d] : 0.f; };
+        auto wx = [&](const float* wp, int d) { return (unsigned)d < (unsigned)w ? wp[d] : 0.f; };
+        uint32_t ah[4], al[4];
+        split_tf32(wy(w0, gq - lr0), ah[0], al[0]);
+        split_tf32(wy(w0, gq + 8 - lr0), ah[1], al[1]);
+        split_tf32(wy(w1, gq - lr1), ah[2], al[2]);
+        split_tf32(wy(w1, gq + 8 - lr1), ah[3], al[3]);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int col = 8 * j + gq;
+          const float x0 = wx(w0, col - lc0), x1 = wx(w1, col - lc1);
+          uint32_t rh0, rl0, rh1, rl1, ih0, il0, ih1, il1;
+          split_tf32(x0 * cr0, rh0, rl0);
+          split_tf32(x1 * cr1, rh1, rl1);
+          split_tf32(x0 * ci0, ih0, il0);
+          split_tf32(x1 * ci1, ih1, il1);
+          mma_tf32(dre[j], ah, rh0, rh1);
+          mma_tf32(dre[j], ah, rl0, rl1);
+          mma_tf32(dre[j], al, rh0, rh1);
+          mma_tf32(dim[j], ah, ih0, ih1);
+          mma_tf32(dim[j], ah, il0, il1);
+          mma_tf32(dim[j], al, ih0, ih1);
+        }
+      }
+      __syncwarp();
+    }
+    // add the subgrid to the band: fragment element e of n-tile j is
+    // (row gq + 8 (e >= 2), col 8 j + 2 t + (e & 1))
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int r = gq + (e >= 2 ? 8 : 0), cc = 8 * j + 2 * t + (e & 1);
+        const float vr = dre[j][e], vi = dim[j][e];
+        if (r >= SG || cc >= SG || (vr == 0.f && vi == 0.f)) continue;
+        int rw = item.z + r, cl = item.w + cc;
+        if (rw >= P.nf2) rw -= P.nf2;
+        if (cl >= P.nf1) cl -= P.nf1;
+        if (rw >= P.b2n || cl >= P.b1n) continue;  // beyond the band: only zero taps land here
+        float* dst = band + 2 * ((size_t)rw * P.b1n + cl);
+        atomicAdd(dst, vr);
+        atomicAdd(dst + 1, vi);
+      }
+    }
+  }
+  if (staged) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 2 * ncell; i += blockDim.x) {
+      const float vv = band[i];
+      if (vv != 0.f) atomicAdd(gband + i, vv);
+    }
+    __syncthreads();
+  }
+}
+
 template <typename R>
 __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
+  if constexpr (std::is_same<R, float>::value) {
+    if (c.P->w <= 9 && c.P->bin == 8) {
+      fg_spread_tc(c, g);
+      return;
+    }
+  }
   const ProbDesc& P = *c.P;
   const R* xu = at<R>(c.base, P.o_u);
   const R* xv = at<R>(c.base, P.o_v);
