@@ -322,6 +322,8 @@ def main():
     ap.add_argument("--target-rtol", type=float, default=1e-4)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="automatic launch shape instead of the autotuner (fewer launches, for profiling)")
     ap.add_argument("--config5", action="store_true",
                     help="also solve the 64-frame movie and the 1024x1024 / 2e6-visibility image")
     ap.add_argument("--warm-problems", type=int, default=256,
@@ -399,8 +401,11 @@ def main():
     # launch shape (CTAs per problem, spreading tile) from the autotuner,
     # timed on short solves of this batch
     from smili_b200 import autotune
-    tuned = autotune.tune(probs, 32, niter=20, repeats=2, device=local,
-                          cands=[(2, 8), (3, 8), (4, 8), (3, 16)])
+    if args.no_autotune:
+        tuned = {"ctas_per_problem": 0, "spread_bin": 8}
+    else:
+        tuned = autotune.tune(probs, 32, niter=20, repeats=2, device=local,
+                              cands=[(2, 8), (3, 8), (4, 8), (3, 16)])
     # FP32 batched, inputs resident on the device: the reference's iteration
     # budget with an early exit at the plain solve's final cost
     opts = _lib.make_options(32, 1e-6, tuned["ctas_per_problem"], local, spread_bin=tuned["spread_bin"])
@@ -478,7 +483,8 @@ def main():
                                    f"plain FP64 solve's final cost x (1 + {args.target_rtol:g})",
                        "batch": B, "distinct_seeds": S,
                        "launch": {"ctas_per_problem": tuned["ctas_per_problem"],
-                                  "spread_bin": tuned["spread_bin"], "chosen_by": "autotuner (20-iteration solves)"},
+                                  "spread_bin": tuned["spread_bin"],
+                                  "chosen_by": "automatic" if args.no_autotune else "autotuner (20-iteration solves)"},
                        "precision": "FP32 transforms + compensated chi-square, FP64 L-BFGS-B",
                        "warm_start": "not applicable to this workload: its station-based gains "
                                      "scramble visibility phases, so no dirty image exists to start "

@@ -99,6 +99,48 @@ __device__ __forceinline__ void dft5(cpx<R>* v) {
   v[3] = csub(r2, q2);
 }
 
+// One radix-RR pass: n/RR butterflies per sequence for S sequences, src ->
+// dst, with Ns the product of the radices already applied.  RR is a
+// template constant so the butterfly's values stay in registers.
+template <int RR, typename R>
+__device__ __forceinline__ void fft_pass(const cpx<R>* src, cpx<R>* dst, int n, int Ns, int S,
+                                         const cpx<R>* __restrict__ tw) {
+  const int nr = n / RR;
+  const int tstep = n / (Ns * RR);
+  // (s, j) = divmod(idx, nr) advanced incrementally as idx steps by
+  // blockDim.x; one division per step (for k = j mod Ns) instead of three
+  int s = threadIdx.x / nr, j = threadIdx.x - (threadIdx.x / nr) * nr;
+  const int ds = blockDim.x / nr, dj = blockDim.x - ds * nr;
+  int jq = j / Ns, k = j - jq * Ns;
+  for (int idx = threadIdx.x; idx < S * nr; idx += blockDim.x) {
+    const cpx<R>* in = src + (size_t)s * n;
+    cpx<R> v[RR];
+#pragma unroll
+    for (int r = 0; r < RR; ++r) v[r] = in[j + r * nr];
+    if (k) {
+#pragma unroll
+      for (int r = 1; r < RR; ++r) v[r] = cmul(v[r], tw[k * r * tstep]);
+    }
+    if constexpr (RR == 8) dft8(v);
+    else if constexpr (RR == 4) dft4(v[0], v[1], v[2], v[3]);
+    else if constexpr (RR == 2) dft2(v);
+    else if constexpr (RR == 3) dft3(v);
+    else dft5(v);
+    cpx<R>* out = dst + (size_t)s * n + jq * Ns * RR + k;
+#pragma unroll
+    for (int r = 0; r < RR; ++r) out[r * Ns] = v[r];
+    // advance to idx + blockDim.x
+    s += ds;
+    j += dj;
+    if (j >= nr) {
+      j -= nr;
+      ++s;
+    }
+    jq = j / Ns;  // Ns is a power of the radices; one division per step
+    k = j - jq * Ns;
+  }
+}
+
 // Transform S sequences (buf[s*n + i]) in shared memory; returns the buffer
 // that holds the result (buf or work).  All threads of the block must call.
 template <typename R>
@@ -110,39 +152,12 @@ __device__ cpx<R>* smem_fft(cpx<R>* buf, cpx<R>* work, const FftPlan& pl, int S,
   int Ns = 1;
   for (int p = 0; p < pl.nrad; ++p) {
     const int Rr = pl.rad[p];
-    const int nr = n / Rr;
-    const int tstep = n / (Ns * Rr);
-    // (s, j) = divmod(idx, nr) advanced incrementally as idx steps by
-    // blockDim.x; one division per step (for k = j mod Ns) instead of three
-    int s = threadIdx.x / nr, j = threadIdx.x - (threadIdx.x / nr) * nr;
-    const int ds = blockDim.x / nr, dj = blockDim.x - ds * nr;
-    int jq = j / Ns, k = j - jq * Ns;
-    for (int idx = threadIdx.x; idx < S * nr; idx += blockDim.x) {
-      const cpx<R>* in = src + (size_t)s * n;
-      cpx<R> v[8];
-      for (int r = 0; r < Rr; ++r) {
-        cpx<R> a = in[j + r * nr];
-        if (r && k) a = cmul(a, tw[k * r * tstep]);
-        v[r] = a;
-      }
-      switch (Rr) {
-        case 8: dft8(v); break;
-        case 4: dft4(v[0], v[1], v[2], v[3]); break;
-        case 2: dft2(v); break;
-        case 3: dft3(v); break;
-        default: dft5(v); break;
-      }
-      cpx<R>* out = dst + (size_t)s * n + jq * Ns * Rr + k;
-      for (int r = 0; r < Rr; ++r) out[r * Ns] = v[r];
-      // advance to idx + blockDim.x
-      s += ds;
-      j += dj;
-      if (j >= nr) {
-        j -= nr;
-        ++s;
-      }
-      jq = j / Ns;  // Ns is a power of the radices; one division per step
-      k = j - jq * Ns;
+    switch (Rr) {
+      case 8: fft_pass<8>(src, dst, n, Ns, S, tw); break;
+      case 4: fft_pass<4>(src, dst, n, Ns, S, tw); break;
+      case 2: fft_pass<2>(src, dst, n, Ns, S, tw); break;
+      case 3: fft_pass<3>(src, dst, n, Ns, S, tw); break;
+      default: fft_pass<5>(src, dst, n, Ns, S, tw); break;
     }
     __syncthreads();
     cpx<R>* t = src;

@@ -168,13 +168,45 @@ __device__ void fg_t2_cols(FgCtx<R>& c, const GroupCtx& g) {
   }
 }
 
-// kernel taps of one point: first cell index and the w weights per axis
-template <typename R>
-__device__ __forceinline__ void taps(R xi, int w, R beta, int& l0, R* k) {
-  const R half = (R)0.5 * (R)w;
-  l0 = (int)ceil(xi - half);
+// Interpolation of the points j = j0, j0 + dj, ... < nuv from the band:
+// V_j = sum_b psi(v_j - l2 - b) sum_a psi(u_j - l1 - a) band[l2 + b][l1 + a].
+// The kernel width W is a template constant so both tap vectors stay in
+// registers and the W row loads of a tap row issue back to back.
+template <int W, typename R>
+__device__ __forceinline__ void interp_points(const ProbDesc& P, const R* __restrict__ xu, const R* __restrict__ xv,
+                                              const cpx<R>* bandA, cpx<R>* V, R beta, int j0, int dj) {
+  const R half = (R)0.5 * (R)W;
   const R inv = (R)1 / half;
-  for (int a = 0; a < w; ++a) k[a] = es_kernel(((R)(l0 + a) - xi) * inv, beta);
+  for (int j = j0; j < P.nuv; j += dj) {
+    const R x1 = xu[j], x2 = xv[j];
+    const int l1 = (int)ceil(x1 - half), l2 = (int)ceil(x2 - half);
+    R k1[W], k2[W];
+#pragma unroll
+    for (int a = 0; a < W; ++a) {
+      k1[a] = es_kernel(((R)(l1 + a) - x1) * inv, beta);
+      k2[a] = es_kernel(((R)(l2 + a) - x2) * inv, beta);
+    }
+    const int c1 = imod(l1 - P.b1s, P.nf1), c2 = imod(l2 - P.b2s, P.nf2);
+    R ar = 0, ai = 0;
+#pragma unroll
+    for (int b = 0; b < W; ++b) {
+      int rw = c2 + b;  // wraps only when the band spans the whole fine grid
+      if (rw >= P.nf2) rw -= P.nf2;
+      const cpx<R>* row = bandA + (size_t)rw * P.b1n;
+      R rr = 0, ri = 0;
+#pragma unroll
+      for (int a = 0; a < W; ++a) {
+        int cl = c1 + a;
+        if (cl >= P.nf1) cl -= P.nf1;
+        const cpx<R> q = row[cl];
+        rr += k1[a] * q.x;
+        ri += k1[a] * q.y;
+      }
+      ar += k2[b] * rr;
+      ai += k2[b] * ri;
+    }
+    V[j] = cmk(ar, ai);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -201,29 +233,15 @@ __device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
       bandA = c.sbuf;
     }
   }
-  for (int j = g.rank * SMILI_THREADS + threadIdx.x; j < P.nuv; j += g.G * SMILI_THREADS) {
-    int l1, l2;
-    R k1[SMILI_MAXW], k2[SMILI_MAXW];
-    taps(xu[j], w, beta, l1, k1);
-    taps(xv[j], w, beta, l2, k2);
-    const int c1 = imod(l1 - P.b1s, P.nf1), c2 = imod(l2 - P.b2s, P.nf2);
-    R ar = 0, ai = 0;
-    for (int b = 0; b < w; ++b) {
-      int rw = c2 + b;  // wraps only when the band spans the whole fine grid
-      if (rw >= P.nf2) rw -= P.nf2;
-      const cpx<R>* row = bandA + (size_t)rw * P.b1n;
-      R rr = 0, ri = 0;
-      for (int a = 0; a < w; ++a) {
-        int cl = c1 + a;
-        if (cl >= P.nf1) cl -= P.nf1;
-        const cpx<R> q = row[cl];
-        rr += k1[a] * q.x;
-        ri += k1[a] * q.y;
-      }
-      ar += k2[b] * rr;
-      ai += k2[b] * ri;
-    }
-    V[j] = cmk(ar, ai);
+  const int j0 = g.rank * SMILI_THREADS + threadIdx.x, dj = g.G * SMILI_THREADS;
+  switch (w) {
+#define SMILI_INTERP_W(W) \
+  case W: interp_points<W>(P, xu, xv, bandA, V, beta, j0, dj); break;
+    SMILI_INTERP_W(2) SMILI_INTERP_W(3) SMILI_INTERP_W(4) SMILI_INTERP_W(5) SMILI_INTERP_W(6)
+    SMILI_INTERP_W(7) SMILI_INTERP_W(8) SMILI_INTERP_W(9) SMILI_INTERP_W(10) SMILI_INTERP_W(11)
+    SMILI_INTERP_W(12) SMILI_INTERP_W(13) SMILI_INTERP_W(14) SMILI_INTERP_W(15)
+    default: interp_points<16>(P, xu, xv, bandA, V, beta, j0, dj); break;  // w <= SMILI_MAXW = 16
+#undef SMILI_INTERP_W
   }
   __syncthreads();
 }

@@ -783,13 +783,16 @@ __device__ int lb_cauchy(LbCtx& c) {
     if (threadIdx.x == 0) c.lred[CR_MODE] = CM_XCP_IS_X;
   } else {
     int pj[SMILI_MAXM_DEV];
-    for (int j = 0; j < col; ++j) pj[j] = lptr(S, m, j);
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) pj[j] = j < col ? lptr(S, m, j) : 0;
     // acc: [0]=f1 [1..2col]=p [2col+1]=nbreak [2col+2]=nfree_nb [2col+3]=notbnded
-    //      [2col+4]=tmin [2col+5]=tmax
+    //      [2col+4]=tmin [2col+5]=tmax; accumulated in scalars and the
+    //      guarded, unrolled column arrays py/ps, packed after the loop
     const int K = col2 + 6;
-    double acc[2 * SMILI_MAXM_DEV + 6];
-    for (int k = 0; k < K; ++k) acc[k] = 0.0;
-    acc[col2 + 4] = 1.0e308;
+    double f1a = 0.0, nbr = 0.0, nfr = 0.0, notb = 0.0, tmn = 1.0e308, tmx = 0.0;
+    double py[SMILI_MAXM_DEV], ps[SMILI_MAXM_DEV];
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) py[j] = ps[j] = 0.0;
     for (int i = c.g->rank * SMILI_THREADS + threadIdx.x; i < 2 * SMILI_NBUCKET; i += c.g->G * SMILI_THREADS)
       ghist[i] = 0;
     for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
@@ -812,24 +815,41 @@ __device__ int lb_cauchy(LbCtx& c) {
         c.d[i] = 0.0;
       } else {
         c.d[i] = neggi;
-        acc[0] -= neggi * neggi;
-        for (int j = 0; j < col; ++j) {
-          acc[1 + j] += c.wy[(size_t)pj[j] * n + i] * neggi;
-          acc[1 + col + j] += c.ws[(size_t)pj[j] * n + i] * neggi;
+        f1a -= neggi * neggi;
+#pragma unroll
+        for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+          if (j < col) {
+            py[j] += c.wy[(size_t)pj[j] * n + i] * neggi;
+            ps[j] += c.ws[(size_t)pj[j] * n + i] * neggi;
+          }
         }
         if (nonneg && neggi < 0.0) {
           const double tb = tl / (-neggi);
-          acc[col2 + 1] += 1.0;
-          acc[col2 + 4] = fmin(acc[col2 + 4], tb);
-          acc[col2 + 5] = fmax(acc[col2 + 5], tb);
+          nbr += 1.0;
+          tmn = fmin(tmn, tb);
+          tmx = fmax(tmx, tb);
           key = (unsigned long long)__double_as_longlong(tb);
         } else {
-          acc[col2 + 2] += 1.0;
-          if (fabs(neggi) > 0.0) acc[col2 + 3] = 1.0;
+          nfr += 1.0;
+          if (fabs(neggi) > 0.0) notb = 1.0;
         }
       }
       c.bkey[i] = key;
     }
+    double acc[2 * SMILI_MAXM_DEV + 6];
+    acc[0] = f1a;
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+      if (j < col) {
+        acc[1 + j] = py[j];
+        acc[1 + col + j] = ps[j];
+      }
+    }
+    acc[col2 + 1] = nbr;
+    acc[col2 + 2] = nfr;
+    acc[col2 + 3] = notb;
+    acc[col2 + 4] = tmn;
+    acc[col2 + 5] = tmx;
     for (int k = threadIdx.x; k < K; k += blockDim.x)
       c.ops[k] = (k == col2 + 3 || k == col2 + 5) ? RED_MAX : (k == col2 + 4 ? RED_MIN : RED_SUM);
     __syncthreads();
@@ -1095,7 +1115,8 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
   const ProbDesc& P = *c.P;
   const int m = c.m, n = c.n, col = S.col, col2 = 2 * col;
   int pj[SMILI_MAXM_DEV];
-  for (int j = 0; j < col; ++j) pj[j] = lptr(S, m, j);
+#pragma unroll
+  for (int j = 0; j < SMILI_MAXM_DEV; ++j) pj[j] = j < col ? lptr(S, m, j) : 0;
   __shared__ double a_s[2 * SMILI_MAXM_DEV], wv_s[2 * SMILI_MAXM_DEV];
   __shared__ int err_s;
   const bool unc = !S.cnstnd && col > 0;
@@ -1110,23 +1131,37 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
   __syncthreads();
   if (err_s) return err_s;
   const double theta = S.theta;
-  double acc[2 * SMILI_MAXM_DEV];
-  for (int k = 0; k < col2; ++k) acc[k] = 0.0;
+  double ay[SMILI_MAXM_DEV], as[SMILI_MAXM_DEV];
+#pragma unroll
+  for (int j = 0; j < SMILI_MAXM_DEV; ++j) ay[j] = as[j] = 0.0;
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     if (unc) {
       c.r[i] = -c.gv[i];
     } else if (c.freef[i]) {
       double ri = -theta * (c.z[i] - c.x[i]) - c.gv[i];
-      for (int j = 0; j < col; ++j)
-        ri += c.wy[(size_t)pj[j] * n + i] * a_s[j] + c.ws[(size_t)pj[j] * n + i] * (theta * a_s[col + j]);
+#pragma unroll
+      for (int j = 0; j < SMILI_MAXM_DEV; ++j)
+        if (j < col)
+          ri += c.wy[(size_t)pj[j] * n + i] * a_s[j] + c.ws[(size_t)pj[j] * n + i] * (theta * a_s[col + j]);
       c.r[i] = ri;
     }
     if (c.freef[i] || unc) {
       const double ri = c.r[i];
-      for (int j = 0; j < col; ++j) {
-        acc[j] += c.wy[(size_t)pj[j] * n + i] * ri;
-        acc[col + j] += c.ws[(size_t)pj[j] * n + i] * ri;
+#pragma unroll
+      for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+        if (j < col) {
+          ay[j] += c.wy[(size_t)pj[j] * n + i] * ri;
+          as[j] += c.ws[(size_t)pj[j] * n + i] * ri;
+        }
       }
+    }
+  }
+  double acc[2 * SMILI_MAXM_DEV];
+#pragma unroll
+  for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+    if (j < col) {
+      acc[j] = ay[j];
+      acc[col + j] = as[j];
     }
   }
   set_ops(c, col2, RED_SUM);
@@ -1154,8 +1189,10 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
     c.xp[i] = c.z[i];
     if (c.freef[i] || unc) {
       double ri = c.r[i];
-      for (int j = 0; j < col; ++j)
-        ri += c.wy[(size_t)pj[j] * n + i] * wv_s[j] / theta + c.ws[(size_t)pj[j] * n + i] * wv_s[col + j];
+#pragma unroll
+      for (int j = 0; j < SMILI_MAXM_DEV; ++j)
+        if (j < col)
+          ri += c.wy[(size_t)pj[j] * n + i] * wv_s[j] / theta + c.ws[(size_t)pj[j] * n + i] * wv_s[col + j];
       ri *= 1.0 / theta;
       c.r[i] = ri;
       if (P.nonneg) {
@@ -1505,21 +1542,36 @@ __device__ int lb_after_fg(LbCtx& c, double f, double gd_fg, double sbg) {
     // matupd (lbfgsb.f:2584-2670) fused with r = g - r, d = stp d and rr
     const int n = c.n, itail = S.itail - 1;
     const double sc = (S.stp == 1.0) ? 1.0 : S.stp;
-    double acc[1 + 2 * SMILI_MAXM_DEV];
     const int K = 1 + 2 * m;
-    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    // per-column partial sums in registers: the column loops are unrolled
+    // to the largest memory with a guard, so no array is indexed at run time
+    double rr_acc = 0.0, ay[SMILI_MAXM_DEV], as[SMILI_MAXM_DEV];
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) ay[j] = as[j] = 0.0;
     for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
       const double ri = c.gv[i] - c.r[i];
       const double di = c.d[i] * sc;
-      acc[0] += ri * ri;
-      for (int j = 0; j < m; ++j) {
-        acc[1 + j] += di * c.wy[(size_t)j * n + i];
-        acc[1 + m + j] += c.ws[(size_t)j * n + i] * di;
+      rr_acc += ri * ri;
+#pragma unroll
+      for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+        if (j < m) {
+          ay[j] += di * c.wy[(size_t)j * n + i];
+          as[j] += c.ws[(size_t)j * n + i] * di;
+        }
       }
       c.ws[(size_t)itail * n + i] = di;
       c.wy[(size_t)itail * n + i] = ri;
       c.r[i] = ri;
       c.d[i] = di;
+    }
+    double acc[1 + 2 * SMILI_MAXM_DEV];
+    acc[0] = rr_acc;
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+      if (j < m) {
+        acc[1 + j] = ay[j];
+        acc[1 + m + j] = as[j];
+      }
     }
     set_ops(c, K, RED_SUM);
     if (!lb_reduce(c, acc, K)) return lb_abort(c);
