@@ -91,6 +91,7 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
   const ProbDesc& P = *c.P;
   const double* x = at<double>(c.base, P.o_x);
   const int* inv = at<int>(c.base, P.o_inv);
+  double* xg = at<double>(c.base, P.o_xg);
   const double* dc1 = at<double>(c.base, P.o_dc1);
   const double* dc2 = at<double>(c.base, P.o_dc2);
   const cpx<R>* tw1 = at<cpx<R>>(c.base, P.o_tw1);
@@ -110,6 +111,7 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
       const int s = i / nx, ix = i - s * nx, iy = row0 + s;
       const int pv = inv[iy * nx + ix];
       const double val = pv >= 0 ? x[pv] : 0.0;
+      xg[(size_t)iy * nx + ix] = val;
       c.sbuf[s * n1 + wrapn(ix - nx / 2, n1)] = cmk<R>((R)(val * dc1[ix] * dc2[iy]), (R)0);
       if (need_mom && pv >= 0) {
         const double fx = ix + 1, fy = iy + 1;  // 1-based pixel numbers as the reference
@@ -268,94 +270,149 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
   const R wf = (R)P.wfcv, wa = (R)P.wamp, wc = (R)P.wcp, wq = (R)P.wca;
   // model_fcv/amp/cp/ca (fftlib.f90:744-1254) also return each datum's model and residual
   double* mres = P.o_model ? at<double>(c.base, P.o_model) : nullptr;
-  for (int i = g.rank * SMILI_THREADS + threadIdx.x; i < e_end; i += g.G * SMILI_THREADS) {
-    const R var = dvar[i];
-    if (i < e_amp) {  // complex visibilities (fftlib.f90:384-439)
-      const int slot = i;
-      const int k = didx[slot];
-      const R sg = (R)dsgn[slot];
-      const cpx<R> Vk = V[k];
-      const R rr = dre[i] - Vk.x, ri = dim[i] - sg * Vk.y;
-      acc[0].add(((rr * rr + ri * ri) / var) * wf);
-      const R factor = (R)-2 / var * wf;
-      contrib[slot] = cmk(factor * rr, factor * ri * sg);
-      if (mres) {
-        mres[4 * i] = Vk.x;
-        mres[4 * i + 1] = sg * Vk.y;
-        mres[4 * i + 2] = rr;
-        mres[4 * i + 3] = ri;
-      }
-    } else if (i < e_cp) {  // amplitudes (fftlib.f90:442-493)
-      const int slot = s_amp + (i - e_amp);
-      const cpx<R> Vk = V[didx[slot]];
-      const R model = sqrt(Vk.x * Vk.x + Vk.y * Vk.y);
-      const R resid = dre[i] - model;
-      acc[1].add((resid * resid / var) * wa);
-      const R factor = (R)-2 * resid / var / model * wa;
-      contrib[slot] = cmk(factor * Vk.x, factor * Vk.y);
-      if (mres) {
-        mres[4 * i] = model;
-        mres[4 * i + 1] = 0;
-        mres[4 * i + 2] = resid;
-        mres[4 * i + 3] = 0;
-      }
-    } else if (i < e_ca) {  // closure phases (fftlib.f90:576-655)
-      const int slot = s_cp + 3 * (i - e_cp);
-      cpx<R> Vq[3];
-      R a2[3], sg[3];
-      R model = 0;
-      for (int q = 0; q < 3; ++q) {
-        Vq[q] = V[didx[slot + q]];
-        sg[q] = (R)dsgn[slot + q];
-        a2[q] = Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y;
-        model = atan2(Vq[q].y, Vq[q].x) * sg[q] + model;
-      }
-      const R resid = dre[i] - model;
-      R sr, cr;
-      if (sizeof(R) == 8) {
-        double s_, c_;
-        sincos((double)resid, &s_, &c_);
-        sr = (R)s_;
-        cr = (R)c_;
-      } else {
-        float s_, c_;
-        sincosf((float)resid, &s_, &c_);
-        sr = (R)s_;
-        cr = (R)c_;
-      }
-      acc[2].add(((R)2 * ((R)1 - cr) / var) * wc);
-      const R factor = (R)-2 * sr / var * wc;
-      for (int q = 0; q < 3; ++q)
-        contrib[slot + q] = cmk(-factor / a2[q] * Vq[q].y * sg[q], factor / a2[q] * Vq[q].x * sg[q]);
-      if (mres) {  // unwrapped; the host wraps both into (-pi, pi] as model_cp does
-        mres[4 * i] = model;
-        mres[4 * i + 1] = 0;
-        mres[4 * i + 2] = resid;
-        mres[4 * i + 3] = 0;
-      }
-    } else {  // log closure amplitudes (fftlib.f90:496-573)
-      const int slot = s_ca + 4 * (i - e_ca);
-      cpx<R> Vq[4];
-      R a[4];
-      for (int q = 0; q < 4; ++q) {
-        Vq[q] = V[didx[slot + q]];
-        a[q] = sqrt(Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y);
-      }
-      const R model = log(a[0]) + log(a[1]) - log(a[2]) - log(a[3]);
-      const R resid = dre[i] - model;
-      acc[3].add((resid * resid / var) * wq);
-      const R factor = (R)-2 * resid / var * wq;
-      for (int q = 0; q < 4; ++q) {
-        const R f = (q < 2 ? factor : -factor) / (a[q] * a[q]);
-        contrib[slot + q] = cmk(f * Vq[q].x, f * Vq[q].y);
-      }
-      if (mres) {
-        mres[4 * i] = model;
-        mres[4 * i + 1] = 0;
-        mres[4 * i + 2] = resid;
-        mres[4 * i + 3] = 0;
-      }
+  // One loop per data type over the same items (i = j0 + k dj) in the same
+  // order as a single loop, two items per step: both items' gathers are
+  // issued before either is evaluated, so their latencies overlap.
+  const int j0 = g.rank * SMILI_THREADS + threadIdx.x, dj = g.G * SMILI_THREADS;
+  auto first = [&](int a) { return a <= j0 ? j0 : j0 + (a - j0 + dj - 1) / dj * dj; };
+  auto put = [&](int i, R model, R model2, R resid, R resid2) {
+    if (mres) {
+      mres[4 * i] = model;
+      mres[4 * i + 1] = model2;
+      mres[4 * i + 2] = resid;
+      mres[4 * i + 3] = resid2;
     }
+  };
+  // complex visibilities (fftlib.f90:384-439)
+  auto fcv = [&](int i, const cpx<R>& Vk, R sg, R var, R yr, R yi) {
+    const R rr = yr - Vk.x, ri = yi - sg * Vk.y;
+    acc[0].add(((rr * rr + ri * ri) / var) * wf);
+    const R factor = (R)-2 / var * wf;
+    contrib[i] = cmk(factor * rr, factor * ri * sg);
+    put(i, Vk.x, sg * Vk.y, rr, ri);
+  };
+  for (int i = first(0); i < e_amp; i += 2 * dj) {
+    const int ib = i + dj;
+    const bool two = ib < e_amp;
+    const int ka = didx[i], kb = two ? didx[ib] : ka;
+    const cpx<R> Va = V[ka], Vb = V[kb];
+    const R sa = (R)dsgn[i], sb = two ? (R)dsgn[ib] : sa;
+    const R va = dvar[i], vb = two ? dvar[ib] : va;
+    const R ra = dre[i], rb = two ? dre[ib] : ra, ia = dim[i], ibm = two ? dim[ib] : ia;
+    fcv(i, Va, sa, va, ra, ia);
+    if (two) fcv(ib, Vb, sb, vb, rb, ibm);
+  }
+  // amplitudes (fftlib.f90:442-493)
+  auto amp = [&](int i, const cpx<R>& Vk, R var, R y) {
+    const int slot = s_amp + (i - e_amp);
+    const R model = sqrt(Vk.x * Vk.x + Vk.y * Vk.y);
+    const R resid = y - model;
+    acc[1].add((resid * resid / var) * wa);
+    const R factor = (R)-2 * resid / var / model * wa;
+    contrib[slot] = cmk(factor * Vk.x, factor * Vk.y);
+    put(i, model, 0, resid, 0);
+  };
+  for (int i = first(e_amp); i < e_cp; i += 2 * dj) {
+    const int ib = i + dj;
+    const bool two = ib < e_cp;
+    const int ka = didx[s_amp + (i - e_amp)], kb = two ? didx[s_amp + (ib - e_amp)] : ka;
+    const cpx<R> Va = V[ka], Vb = V[kb];
+    const R va = dvar[i], vb = two ? dvar[ib] : va;
+    const R ya = dre[i], yb = two ? dre[ib] : ya;
+    amp(i, Va, va, ya);
+    if (two) amp(ib, Vb, vb, yb);
+  }
+  // closure phases (fftlib.f90:576-655)
+  auto cp = [&](int i, const cpx<R> (&Vq)[3], const R (&sg)[3], R var, R y) {
+    const int slot = s_cp + 3 * (i - e_cp);
+    R a2[3];
+    R model = 0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      a2[q] = Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y;
+      model = atan2(Vq[q].y, Vq[q].x) * sg[q] + model;
+    }
+    const R resid = y - model;
+    R sr, cr;
+    if (sizeof(R) == 8) {
+      double s_, c_;
+      sincos((double)resid, &s_, &c_);
+      sr = (R)s_;
+      cr = (R)c_;
+    } else {
+      float s_, c_;
+      sincosf((float)resid, &s_, &c_);
+      sr = (R)s_;
+      cr = (R)c_;
+    }
+    acc[2].add(((R)2 * ((R)1 - cr) / var) * wc);
+    const R factor = (R)-2 * sr / var * wc;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+      contrib[slot + q] = cmk(-factor / a2[q] * Vq[q].y * sg[q], factor / a2[q] * Vq[q].x * sg[q]);
+    put(i, model, 0, resid, 0);  // unwrapped; the host wraps both into (-pi, pi] as model_cp does
+  };
+  for (int i = first(e_cp); i < e_ca; i += 2 * dj) {
+    const int ib = i + dj;
+    const bool two = ib < e_ca;
+    const int sa = s_cp + 3 * (i - e_cp), sb = two ? s_cp + 3 * (ib - e_cp) : sa;
+    int ka[3], kb[3];
+    cpx<R> Va[3], Vb[3];
+    R ga[3], gb[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      ka[q] = didx[sa + q];
+      kb[q] = didx[sb + q];
+      ga[q] = (R)dsgn[sa + q];
+      gb[q] = (R)dsgn[sb + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      Va[q] = V[ka[q]];
+      Vb[q] = V[kb[q]];
+    }
+    const R va = dvar[i], vb = two ? dvar[ib] : va;
+    const R ya = dre[i], yb = two ? dre[ib] : ya;
+    cp(i, Va, ga, va, ya);
+    if (two) cp(ib, Vb, gb, vb, yb);
+  }
+  // log closure amplitudes (fftlib.f90:496-573)
+  auto ca = [&](int i, const cpx<R> (&Vq)[4], R var, R y) {
+    const int slot = s_ca + 4 * (i - e_ca);
+    R a[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a[q] = sqrt(Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y);
+    const R model = log(a[0]) + log(a[1]) - log(a[2]) - log(a[3]);
+    const R resid = y - model;
+    acc[3].add((resid * resid / var) * wq);
+    const R factor = (R)-2 * resid / var * wq;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const R f = (q < 2 ? factor : -factor) / (a[q] * a[q]);
+      contrib[slot + q] = cmk(f * Vq[q].x, f * Vq[q].y);
+    }
+    put(i, model, 0, resid, 0);
+  };
+  for (int i = first(e_ca); i < e_end; i += 2 * dj) {
+    const int ib = i + dj;
+    const bool two = ib < e_end;
+    const int sa = s_ca + 4 * (i - e_ca), sb = two ? s_ca + 4 * (ib - e_ca) : sa;
+    int ka[4], kb[4];
+    cpx<R> Va[4], Vb[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      ka[q] = didx[sa + q];
+      kb[q] = didx[sb + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      Va[q] = V[ka[q]];
+      Vb[q] = V[kb[q]];
+    }
+    const R va = dvar[i], vb = two ? dvar[ib] : va;
+    const R ya = dre[i], yb = two ? dre[ib] : ya;
+    ca(i, Va, va, ya);
+    if (two) ca(ib, Vb, vb, yb);
   }
   for (int q = 0; q < 4; ++q) chi[q] += acc[q].value();
 }
@@ -718,39 +775,54 @@ __device__ void fg_t1_cols(FgCtx<R>& c, const GroupCtx& g) {
 // projected-gradient infinity norm used by the optimiser.
 // mom: reduced image moments from F1 (only when tfd/cen/sm are active).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double px(const double* x, const int* inv, int nx, int ny, int ix, int iy) {
-  if (ix < 0 || iy < 0 || ix >= nx || iy >= ny) return 0.0;
-  const int p = inv[iy * nx + ix];
-  return p >= 0 ? x[p] : 0.0;
-}
-
-__device__ double tv_grade_px(const double* x, const int* inv, int nx, int ny, int i1, int j1) {
+// Image value at grid cell (ix, iy), 0 outside the image or at a pixel the
+// solve does not include: through the pixel map (PxMap) or from the dense
+// image grid that the type-2 row pass writes (PxGrid).
+struct PxMap {
+  const double* x;
+  const int* inv;
+  int nx, ny;
+  __device__ __forceinline__ double operator()(int ix, int iy) const {
+    if (ix < 0 || iy < 0 || ix >= nx || iy >= ny) return 0.0;
+    const int p = inv[iy * nx + ix];
+    return p >= 0 ? x[p] : 0.0;
+  }
+};
+struct PxGrid {
+  const double* xg;
+  int nx, ny;
+  __device__ __forceinline__ double operator()(int ix, int iy) const {
+    if (ix < 0 || iy < 0 || ix >= nx || iy >= ny) return 0.0;
+    return xg[(size_t)iy * nx + ix];
+  }
+};
+template <class PX>
+__device__ __forceinline__ double tv_grade_px(const PX& px, int nx, int ny, int i1, int j1) {
   // image.f90:512-612 with 0-based (i1, j1); reproduces the gradient reset
   double gr = 0.0;
-  const double I11 = px(x, inv, nx, ny, i1, j1);
-  double dIx = (i1 + 1 >= nx) ? 0.0 : px(x, inv, nx, ny, i1 + 1, j1) - I11;
-  double dIy = (j1 + 1 >= ny) ? 0.0 : px(x, inv, nx, ny, i1, j1 + 1) - I11;
+  const double I11 = px(i1, j1);
+  double dIx = (i1 + 1 >= nx) ? 0.0 : px(i1 + 1, j1) - I11;
+  double dIy = (j1 + 1 >= ny) ? 0.0 : px(i1, j1 + 1) - I11;
   double e = sqrt(dIx * dIx + dIy * dIy);
   if (e > 1e-10) gr -= (dIx + dIy) / e;
   if (i1 - 1 >= 0) {
-    const double I01 = px(x, inv, nx, ny, i1 - 1, j1);
+    const double I01 = px(i1 - 1, j1);
     dIx = I11 - I01;
-    dIy = (j1 + 1 >= ny) ? 0.0 : px(x, inv, nx, ny, i1 - 1, j1 + 1) - I01;
+    dIy = (j1 + 1 >= ny) ? 0.0 : px(i1 - 1, j1 + 1) - I01;
     e = sqrt(dIx * dIx + dIy * dIy);
     if (e > 1e-10) gr += dIx / e;
     else gr = 0.0;
   }
   if (j1 - 1 >= 0) {
-    const double I10 = px(x, inv, nx, ny, i1, j1 - 1);
+    const double I10 = px(i1, j1 - 1);
     dIy = I11 - I10;
-    dIx = (i1 + 1 >= nx) ? 0.0 : px(x, inv, nx, ny, i1 + 1, j1 - 1) - I10;
+    dIx = (i1 + 1 >= nx) ? 0.0 : px(i1 + 1, j1 - 1) - I10;
     e = sqrt(dIx * dIx + dIy * dIy);
     if (e > 1e-10) gr += dIy / e;
     else gr = 0.0;
   }
   return gr;
 }
-
 struct RegMoments {
   double Isum_abs, xcen, ycen, Sg[3], mom[2], Sp[3];
   double tfd_resid;
@@ -797,11 +869,10 @@ __device__ void frame_moments(const ProbDesc& P, char* base, double (&mom)[10]) 
   }
 }
 
-__device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, const RegMoments& rm,
-                            int lo, int hi, double (&reg)[8], double& gd, double& sbg,
-                            bool opt_terms = true) {
+template <class PX>
+__device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const RegMoments& rm, int lo, int hi,
+                              double (&reg)[8], double& gd, double& sbg, bool opt_terms) {
   const double* x = at<double>(base, P.o_x);
-  const int* inv = at<int>(base, P.o_inv);
   const int* xi = at<int>(base, P.o_xidx);
   const int* yi = at<int>(base, P.o_yidx);
   const double* gchi = at<double>(base, P.o_gchi);
@@ -813,6 +884,9 @@ __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, co
   const double* klw = P.has_kl ? at<double>(base, P.o_klw) : nullptr;
   const double* gsw = P.has_gs ? at<double>(base, P.o_gsw) : nullptr;
   const int nx = P.nx, ny = P.ny;
+  // running sums in registers (the caller's accumulators are written once
+  // at the end, so the stores of the loop cannot alias them)
+  double r0 = reg[0], r1 = reg[1], r2 = reg[2], r3 = reg[3], r4 = reg[4], gdl = gd, sbgl = sbg;
   for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
     const int ix = xi[p], iy = yi[p];
     const double I = x[p];
@@ -828,33 +902,33 @@ __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, co
     }
     if (P.has_l1) {
       const double a = smabs(I);
-      reg[0] += P.l1_l * l1w[p] * a;
+      r0 += P.l1_l * l1w[p] * a;
       gr += P.l1_l * l1w[p] * (I / a);
     }
     if (P.has_kl) {
       const double a = smabs(I), pr = klw[p];
-      reg[3] += P.kl_l * (a * log(a / pr) + pr / 2.718281828459045235);
+      r3 += P.kl_l * (a * log(a / pr) + pr / 2.718281828459045235);
       gr += P.kl_l * (I / a) * (log(a / pr) + 1);
     }
     if (P.has_gs) {
       const double a = smabs(I), pr = gsw[p];
-      reg[4] += P.gs_l * (a * (log(a / pr) - 1) + pr);
+      r4 += P.gs_l * (a * (log(a / pr) - 1) + pr);
       gr += P.gs_l * (I / a) * log(a / pr);
     }
     if (P.has_tv || P.has_tsv) {
-      const double dIx = (ix + 1 >= nx) ? 0.0 : px(x, inv, nx, ny, ix + 1, iy) - I;
-      const double dIy = (iy + 1 >= ny) ? 0.0 : px(x, inv, nx, ny, ix, iy + 1) - I;
+      const double dIx = (ix + 1 >= nx) ? 0.0 : px(ix + 1, iy) - I;
+      const double dIy = (iy + 1 >= ny) ? 0.0 : px(ix, iy + 1) - I;
       if (P.has_tv) {
-        reg[1] += P.tv_l * tvw[p] * sqrt(dIx * dIx + dIy * dIy);
-        gr += P.tv_l * tvw[p] * tv_grade_px(x, inv, nx, ny, ix, iy);
+        r1 += P.tv_l * tvw[p] * sqrt(dIx * dIx + dIy * dIy);
+        gr += P.tv_l * tvw[p] * tv_grade_px(px, nx, ny, ix, iy);
       }
       if (P.has_tsv) {
-        reg[2] += P.tsv_l * tsvw[p] * (dIx * dIx + dIy * dIy);
+        r2 += P.tsv_l * tsvw[p] * (dIx * dIx + dIy * dIy);
         double gt = 0.0;
-        if (ix + 1 < nx) gt -= 2 * (px(x, inv, nx, ny, ix + 1, iy) - I);
-        if (iy + 1 < ny) gt -= 2 * (px(x, inv, nx, ny, ix, iy + 1) - I);
-        if (ix - 1 >= 0) gt += 2 * (I - px(x, inv, nx, ny, ix - 1, iy));
-        if (iy - 1 >= 0) gt += 2 * (I - px(x, inv, nx, ny, ix, iy - 1));
+        if (ix + 1 < nx) gt -= 2 * (px(ix + 1, iy) - I);
+        if (iy + 1 < ny) gt -= 2 * (px(ix, iy + 1) - I);
+        if (ix - 1 >= 0) gt += 2 * (I - px(ix - 1, iy));
+        if (iy - 1 >= 0) gt += 2 * (I - px(ix, iy - 1));
         gr += P.tsv_l * tsvw[p] * gt;
       }
     }
@@ -871,10 +945,32 @@ __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, co
     const double gv = gchi[(size_t)iy * nx + ix] + gr;
     gout[p] = gv;
     if (!opt_terms) continue;  // a movie frame: the movie pass forms g.d and the projected gradient
-    gd += gv * d[p];
+    gdl += gv * d[p];
     // projected gradient (projgr, lbfgsb.f:2942-2990) with lower bound 0
     double gi = gv;
     if (P.nonneg && gi >= 0.0) gi = fmin(I, gi);
-    sbg = fmax(sbg, fabs(gi));
+    sbgl = fmax(sbgl, fabs(gi));
+  }
+  reg[0] = r0;
+  reg[1] = r1;
+  reg[2] = r2;
+  reg[3] = r3;
+  reg[4] = r4;
+  gd = gdl;
+  sbg = sbgl;
+}
+
+// F8: regularizer values and the full gradient g = grad chi2 + grad reg over
+// pixels [lo, hi); neighbours come from the dense image grid when F1 wrote
+// it in this evaluation (frames without data use the pixel map).
+__device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, const RegMoments& rm,
+                            int lo, int hi, double (&reg)[8], double& gd, double& sbg,
+                            bool opt_terms = true) {
+  if (P.nuv > 0 && P.o_xg) {
+    const PxGrid px{at<double>(base, P.o_xg), P.nx, P.ny};
+    reg_grad_loop(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
+  } else {
+    const PxMap px{at<double>(base, P.o_x), at<int>(base, P.o_inv), P.nx, P.ny};
+    reg_grad_loop(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
   }
 }

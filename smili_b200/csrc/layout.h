@@ -58,6 +58,7 @@ struct ProbDesc {
   double ftarget;          // stop once f <= ftarget at a completed iteration (-inf: off)
   // byte offsets in the arena (0 = absent)
   int64_t o_x0, o_xidx, o_yidx, o_inv;
+  int64_t o_xg;                         // dense image grid [ny][nx] (double), written by F1
   int64_t o_l1w, o_tvw, o_tsvw, o_klw, o_gsw;
   int64_t o_dc1, o_dc2, o_tw1, o_tw2;   // deconvolution factors, twiddle tables
   int64_t o_u, o_v;                     // fine-grid coordinates xi = u n / 2pi (R)

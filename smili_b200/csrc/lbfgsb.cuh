@@ -973,80 +973,89 @@ __device__ int lb_cauchy(LbCtx& c) {
 // ---------------------------------------------------------------------------
 // formk (lbfgsb.f:1848-2172) from Gram sums over the free/active sets
 // ---------------------------------------------------------------------------
+// One FP64 tensor-core product D = A B + D of an 8x4 by 4x8 tile
+// (mma.sync m8n8k4 f64).  Lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4) + {0,1}].
+__device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 __device__ int lb_formk(LbCtx& c) {
   LbState& S = *c.S;
   const int m = c.m, n = c.n, col = S.col;
   // entries: Fyy (a<=b), Ass (a<=b), Fsy (a,b), Asy (a,b) over physical columns
   const int nsym = m * (m + 1) / 2;
   const int E = 2 * nsym + 2 * m * m;
-  const int tpe = SMILI_THREADS / E;  // threads per entry (>= 2 for m <= 6)
-  // tile staging: TE elements x (2m values + flag)
-  const int TE = 256;
-  double* tile = reinterpret_cast<double*>(c.dyn);  // [TE][2m+1] (<= 26 KB)
-  const int stride = 2 * m + 1;
-  const int my_e = threadIdx.x / tpe, my_sub = threadIdx.x % tpe;
-  int kind = -1, ea = 0, eb = 0;
-  if (my_e < E) {
-    int e = my_e;
-    if (e < nsym) {
-      kind = 0;
-    } else if (e < 2 * nsym) {
-      kind = 1;
-      e -= nsym;
-    } else if (e < 2 * nsym + m * m) {
-      kind = 2;
-      e -= 2 * nsym;
-    } else {
-      kind = 3;
-      e -= 2 * nsym + m * m;
+  // The four masked Gram blocks W' diag(mask) W over this CTA's pixels on
+  // the FP64 tensor cores: per 4 pixels, A = (masked column a at pixel k),
+  // B = (column b at pixel k); lane (a = l/4, k = l%4) holds the same
+  // element of both operands, so one load per matrix feeds both.
+  //   Fyy = Y'FY, Fsy = S'FY (free pixels), Ass = S'AS, Asy = S'AY (active)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ca = lane >> 2, pk = lane & 3;
+  const bool cval = ca < m;  // m <= 6 < 8: one 8x8 tile per block
+  const double* wyc = c.wy + (size_t)(cval ? ca : 0) * n;
+  const double* wsc = c.ws + (size_t)(cval ? ca : 0) * n;
+  double fyy[2] = {0.0, 0.0}, fsy[2] = {0.0, 0.0}, ass[2] = {0.0, 0.0}, asy[2] = {0.0, 0.0};
+  const int nchunk = (c.hi - c.lo + 3) >> 2;
+  constexpr int U = 4;  // chunks in flight per warp
+  for (int q0 = warp; q0 < nchunk; q0 += U * nw) {
+    double y[U], sv[U];
+    bool fr[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = c.lo + 4 * (q0 + u * nw) + pk;
+      const bool ok = i < c.hi;  // q0 + u*nw < nchunk whenever i < hi
+      y[u] = (ok && cval) ? wyc[i] : 0.0;
+      sv[u] = (ok && cval) ? wsc[i] : 0.0;
+      fr[u] = ok && c.freef[i] != 0;
     }
-    if (kind < 2) {  // triangular index -> (a, b), a <= b
-      int a = 0;
-      while (e >= m - a) {
-        e -= m - a;
-        ++a;
-      }
-      ea = a;
-      eb = a + e;
-    } else {
-      ea = e / m;
-      eb = e % m;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const double yf = fr[u] ? y[u] : 0.0, sf = fr[u] ? sv[u] : 0.0, sa = fr[u] ? 0.0 : sv[u];
+      dmma_884(fyy, yf, y[u]);
+      dmma_884(fsy, sf, y[u]);
+      dmma_884(ass, sa, sv[u]);
+      dmma_884(asy, sa, y[u]);
     }
   }
-  double accv = 0.0;
-  for (int t0 = c.lo; t0 < c.hi; t0 += TE) {
-    const int cnt = min(TE, c.hi - t0);
-    for (int q = threadIdx.x; q < cnt * stride; q += blockDim.x) {
-      const int el = q / stride, k = q - el * stride, i = t0 + el;
-      double v;
-      if (k < m) v = c.wy[(size_t)k * n + i];
-      else if (k < 2 * m) v = c.ws[(size_t)(k - m) * n + i];
-      else v = (double)c.freef[i];
-      tile[el * stride + k] = v;
-    }
-    __syncthreads();
-    if (kind >= 0) {
-      for (int el = my_sub; el < cnt; el += tpe) {
-        const double* row = tile + el * stride;
-        const bool fr = row[2 * m] > 0.5;
-        switch (kind) {
-          case 0: if (fr) accv += row[ea] * row[eb]; break;
-          case 1: if (!fr) accv += row[m + ea] * row[m + eb]; break;
-          case 2: if (fr) accv += row[m + ea] * row[eb]; break;
-          default: if (!fr) accv += row[m + ea] * row[eb]; break;
-        }
-      }
-    }
-    __syncthreads();
-  }
-  // combine the tpe partials of each entry in fixed order
+  // combine the warps' tiles in fixed order: part[warp][tile][8x8]
   double* part = reinterpret_cast<double*>(c.dyn);
-  part[threadIdx.x] = accv;
+  {
+    double* pw = part + (size_t)warp * 4 * 64 + ca * 8 + 2 * pk;
+    pw[0] = fyy[0];
+    pw[1] = fyy[1];
+    pw[64] = fsy[0];
+    pw[65] = fsy[1];
+    pw[128] = ass[0];
+    pw[129] = ass[1];
+    pw[192] = asy[0];
+    pw[193] = asy[1];
+  }
   __syncthreads();
   for (int e = threadIdx.x; e < E; e += blockDim.x) {
-    double s = 0.0;
-    for (int q = 0; q < tpe; ++q) s += part[e * tpe + q];
-    c.red[e] = s;
+    int t, a, b;
+    if (e < 2 * nsym) {  // triangular index -> (a, b), a <= b
+      t = e < nsym ? 0 : 2;
+      int r = e < nsym ? e : e - nsym;
+      a = 0;
+      while (r >= m - a) {
+        r -= m - a;
+        ++a;
+      }
+      b = a + r;
+    } else {
+      const int r = e - 2 * nsym;
+      t = r < m * m ? 1 : 3;
+      const int q = r < m * m ? r : r - m * m;
+      a = q / m;
+      b = q % m;
+    }
+    double sum = 0.0;
+    for (int w = 0; w < nw; ++w) sum += part[(size_t)w * 256 + t * 64 + a * 8 + b];
+    c.red[e] = sum;
   }
   for (int k = threadIdx.x; k < E; k += blockDim.x) c.ops[k] = RED_SUM;
   __syncthreads();
@@ -1135,24 +1144,29 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
 #pragma unroll
   for (int j = 0; j < SMILI_MAXM_DEV; ++j) ay[j] = as[j] = 0.0;
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
+    if (!unc && !c.freef[i]) continue;
+    // the row of W at pixel i, loaded once for r_i and for W'Z r
+    double wyv[SMILI_MAXM_DEV], wsv[SMILI_MAXM_DEV];
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+      wyv[j] = j < col ? c.wy[(size_t)pj[j] * n + i] : 0.0;
+      wsv[j] = j < col ? c.ws[(size_t)pj[j] * n + i] : 0.0;
+    }
+    double ri;
     if (unc) {
-      c.r[i] = -c.gv[i];
-    } else if (c.freef[i]) {
-      double ri = -theta * (c.z[i] - c.x[i]) - c.gv[i];
+      ri = -c.gv[i];
+    } else {
+      ri = -theta * (c.z[i] - c.x[i]) - c.gv[i];
 #pragma unroll
       for (int j = 0; j < SMILI_MAXM_DEV; ++j)
-        if (j < col)
-          ri += c.wy[(size_t)pj[j] * n + i] * a_s[j] + c.ws[(size_t)pj[j] * n + i] * (theta * a_s[col + j]);
-      c.r[i] = ri;
+        if (j < col) ri += wyv[j] * a_s[j] + wsv[j] * (theta * a_s[col + j]);
     }
-    if (c.freef[i] || unc) {
-      const double ri = c.r[i];
+    c.r[i] = ri;
 #pragma unroll
-      for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
-        if (j < col) {
-          ay[j] += c.wy[(size_t)pj[j] * n + i] * ri;
-          as[j] += c.ws[(size_t)pj[j] * n + i] * ri;
-        }
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+      if (j < col) {
+        ay[j] += wyv[j] * ri;
+        as[j] += wsv[j] * ri;
       }
     }
   }
@@ -1185,26 +1199,35 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
   if (err_s) return err_s;
   // d := (d + W wv) / theta on the free set, then project z + d
   double acc2[2] = {0.0, 0.0};  // iword (max), dd_p (sum)
+  double wq[SMILI_MAXM_DEV], wr[SMILI_MAXM_DEV];
+#pragma unroll
+  for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+    wq[j] = j < col ? wv_s[j] : 0.0;
+    wr[j] = j < col ? wv_s[col + j] : 0.0;
+  }
+  const double rtheta = 1.0 / theta;
+  // one pass: d, the projected z and the directional derivative (z - x).g
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
-    c.xp[i] = c.z[i];
+    const double zi = c.z[i];
+    c.xp[i] = zi;
+    double zn = zi;
     if (c.freef[i] || unc) {
       double ri = c.r[i];
 #pragma unroll
       for (int j = 0; j < SMILI_MAXM_DEV; ++j)
-        if (j < col)
-          ri += c.wy[(size_t)pj[j] * n + i] * wv_s[j] / theta + c.ws[(size_t)pj[j] * n + i] * wv_s[col + j];
-      ri *= 1.0 / theta;
+        if (j < col) ri += c.wy[(size_t)pj[j] * n + i] * wq[j] / theta + c.ws[(size_t)pj[j] * n + i] * wr[j];
+      ri *= rtheta;
       c.r[i] = ri;
       if (P.nonneg) {
-        const double zk = fmax(0.0, c.z[i] + ri);
-        c.z[i] = zk;
-        if (zk == 0.0) acc2[0] = 1.0;
+        zn = fmax(0.0, zi + ri);
+        if (zn == 0.0) acc2[0] = 1.0;
       } else {
-        c.z[i] = c.z[i] + ri;
+        zn = zi + ri;
       }
+      c.z[i] = zn;
     }
+    acc2[1] += (zn - c.x[i]) * c.gv[i];
   }
-  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) acc2[1] += (c.z[i] - c.x[i]) * c.gv[i];
   if (threadIdx.x == 0) {
     c.ops[0] = RED_MAX;
     c.ops[1] = RED_SUM;

@@ -878,6 +878,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.o_bandC = ar.take(C * (size_t)d.b2n * d.b1n);
   d.o_tmpC = ar.take(C * (size_t)d.b2n * nx);
   d.o_gchi = ar.take(sizeof(double) * (size_t)nx * ny);
+  d.o_xg = ar.take(sizeof(double) * (size_t)nx * ny);
   if (!frame) {
     d.o_x = ar.take(sizeof(double) * N);
     d.o_g = ar.take(sizeof(double) * N);
