@@ -405,7 +405,7 @@ def main():
         tuned = {"ctas_per_problem": 0, "spread_bin": 8}
     else:
         tuned = autotune.tune(probs, 32, niter=20, repeats=2, device=local,
-                              cands=[(2, 8), (3, 8), (4, 8), (3, 16)])
+                              cands=[(1, 8), (2, 8), (3, 8)])
     # FP32 batched, inputs resident on the device: the reference's iteration
     # budget with an early exit at the plain solve's final cost
     opts = _lib.make_options(32, 1e-6, tuned["ctas_per_problem"], local, spread_bin=tuned["spread_bin"])

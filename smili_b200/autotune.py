@@ -29,7 +29,7 @@ def candidates(nprob, precision, max_res=None):
     """(ctas_per_problem, spread_bin) pairs worth timing for nprob problems:
     group sizes from one CTA per problem up to the size that still keeps
     every problem resident, times both tile sides."""
-    max_res = max_res or (444 if precision == 32 else 296)
+    max_res = max_res or 296  # two CTAs per SM in both precisions (512 threads FP32, 256 FP64)
     gs = sorted({g for g in (1, 2, 3, 4, 6, 8, 12, 16) if g * nprob <= 2 * max_res} | {1})
     return [(g, b) for g in gs for b in (8, 16)]
 

@@ -7,8 +7,20 @@
 
 #include "layout.h"
 
-#define SMILI_THREADS 256
-#define SMILI_WARPS (SMILI_THREADS / 32)
+// CTA shape of the solver kernel per precision.  FP32 runs 512 threads
+// (two CTAs per SM at 64 registers: 32 resident warps to hide the latency of
+// the gather-heavy stages), FP64 256 threads (two CTAs per SM at 128
+// registers; its shared-memory staging is twice as large).  Device code
+// strides by blockDim.x; buffers shared by both shapes are sized for the
+// larger one.
+template <typename R>
+struct Shape {
+  static constexpr int threads = sizeof(R) == 4 ? 512 : 256;
+  static constexpr int warps = threads / 32;
+  static constexpr int min_blocks = 2;
+};
+#define SMILI_MAX_THREADS 512
+#define SMILI_MAX_WARPS (SMILI_MAX_THREADS / 32)
 
 template <typename R>
 struct cpx {
@@ -58,7 +70,7 @@ __device__ __forceinline__ double red_op(double a, double b, int op) {
 }
 
 // Reduce v[0..K) over the block; result valid in every thread's out[].
-// scratch: SMILI_WARPS * K doubles of shared memory.
+// scratch: (blockDim.x / 32) * K doubles of shared memory.
 template <int K>
 __device__ __forceinline__ void block_reduce(const double (&v)[K], const int (&op)[K],
                                              double (&out)[K], double* scratch) {
@@ -74,7 +86,7 @@ __device__ __forceinline__ void block_reduce(const double (&v)[K], const int (&o
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     double a = scratch[k];
-    for (int w = 1; w < SMILI_WARPS; ++w) a = red_op(a, scratch[w * K + k], op[k]);
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) a = red_op(a, scratch[w * K + k], op[k]);
     out[k] = a;
   }
   __syncthreads();
@@ -199,7 +211,7 @@ __device__ bool group_reduce(GroupCtx& g, double* vals, const unsigned char* ops
 }
 
 // Block reduction of K per-thread values (v[k] in each thread, op per entry)
-// into shared out[0..K).  scratch: SMILI_WARPS * K doubles.
+// into shared out[0..K).  scratch: (blockDim.x / 32) * K doubles.
 __device__ void block_reduce_arr(const double* v, const unsigned char* ops, int K, double* out,
                                  double* scratch) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -212,7 +224,7 @@ __device__ void block_reduce_arr(const double* v, const unsigned char* ops, int 
   __syncthreads();
   for (int k = threadIdx.x; k < K; k += blockDim.x) {
     double a = scratch[k];
-    for (int w = 1; w < SMILI_WARPS; ++w) a = red_op(a, scratch[w * K + k], ops[k]);
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) a = red_op(a, scratch[w * K + k], ops[k]);
     out[k] = a;
   }
   __syncthreads();

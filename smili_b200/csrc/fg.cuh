@@ -44,7 +44,7 @@ __device__ __forceinline__ double smabs(double x) { return sqrt(x * x + 1e-10); 
 
 // rows (sequences) per CTA pass for an FFT of length n
 __device__ __forceinline__ int fft_batch(int n) {
-  int s = (SMILI_THREADS * 8) / n;
+  int s = (int)(blockDim.x * 8) / n;
   return s < 1 ? 1 : s;
 }
 
@@ -100,7 +100,7 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
   const int n1 = P.nf1, nx = P.nx, ny = P.ny;
   const FftPlan pl = make_plan(n1);
   const int S = min(fft_batch(n1), c.smem_cpx / n1);
-  for (int i = g.rank * SMILI_THREADS + threadIdx.x; i < P.b2n * P.b1n; i += g.G * SMILI_THREADS)
+  for (int i = g.rank * blockDim.x + threadIdx.x; i < P.b2n * P.b1n; i += g.G * blockDim.x)
     bandC[i] = cmk<R>(0, 0);
   const bool need_mom = P.has_tfd || P.has_cen || P.has_sm;
   for (int row0 = g.rank * S; row0 < ny; row0 += g.G * S) {
@@ -229,13 +229,13 @@ __device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
   const cpx<R>* bandA = gband;
   if (staged) {
     // only CTAs that own points load the band
-    if (g.rank * SMILI_THREADS < P.nuv) {
+    if (g.rank * (int)blockDim.x < P.nuv) {
       for (int i = threadIdx.x; i < ncell; i += blockDim.x) c.sbuf[i] = gband[i];
       __syncthreads();
       bandA = c.sbuf;
     }
   }
-  const int j0 = g.rank * SMILI_THREADS + threadIdx.x, dj = g.G * SMILI_THREADS;
+  const int j0 = g.rank * blockDim.x + threadIdx.x, dj = g.G * blockDim.x;
   switch (w) {
 #define SMILI_INTERP_W(W) \
   case W: interp_points<W>(P, xu, xv, bandA, V, beta, j0, dj); break;
@@ -273,7 +273,7 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
   // One loop per data type over the same items (i = j0 + k dj) in the same
   // order as a single loop, two items per step: both items' gathers are
   // issued before either is evaluated, so their latencies overlap.
-  const int j0 = g.rank * SMILI_THREADS + threadIdx.x, dj = g.G * SMILI_THREADS;
+  const int j0 = g.rank * blockDim.x + threadIdx.x, dj = g.G * blockDim.x;
   auto first = [&](int a) { return a <= j0 ? j0 : j0 + (a - j0 + dj - 1) / dj * dj; };
   auto put = [&](int i, R model, R model2, R resid, R resid2) {
     if (mres) {
@@ -468,6 +468,29 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// Sum of the chi-square derivative contributions of one uv point: its
+// entries ent[e0..e1) in the contribution slots, added in entry order.  Four
+// entries are fetched per step so their two dependent loads overlap.
+template <typename R>
+__device__ __forceinline__ void gather_contrib(const int* __restrict__ ent, const cpx<R>* __restrict__ contrib,
+                                               int e0, int e1, R& cre, R& cim) {
+  for (int e = e0; e < e1; e += 4) {
+    int k[4];
+    cpx<R> q[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) k[u] = e + u < e1 ? ent[e + u] : -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) q[u] = k[u] >= 0 ? contrib[k[u]] : cmk<R>(0, 0);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (k[u] >= 0) {
+        cre += q[u].x;
+        cim += q[u].y;
+      }
+    }
+  }
+}
+
 __device__ void fg_spread_tc(FgCtx<float>& c, const GroupCtx& g) {
   const ProbDesc& P = *c.P;
   const float* xu = at<float>(c.base, P.o_u);
@@ -506,12 +529,7 @@ __device__ void fg_spread_tc(FgCtx<float>& c, const GroupCtx& g) {
       int lr_l = 0, lc_l = 0;
       float* wr = wtab + lane * 2 * w;
       if (jl < item.y) {
-        const int e1 = off[jl + 1];
-        for (int e = off[jl]; e < e1; ++e) {
-          const cpx<float> q = contrib[ent[e]];
-          cre_l += q.x;
-          cim_l += q.y;
-        }
+        gather_contrib(ent, contrib, off[jl], off[jl + 1], cre_l, cim_l);
         cim_l = -cim_l;  // c = Vresre - i Vresim
         const float xi1 = xu[jl], xi2 = xv[jl];
         const int l1 = (int)ceilf(xi1 - half), l2 = (int)ceilf(xi2 - half);
@@ -575,8 +593,12 @@ __device__ void fg_spread_tc(FgCtx<float>& c, const GroupCtx& g) {
         if (cl >= P.nf1) cl -= P.nf1;
         if (rw >= P.b2n || cl >= P.b1n) continue;  // beyond the band: only zero taps land here
         float* dst = band + 2 * ((size_t)rw * P.b1n + cl);
-        atomicAdd(dst, vr);
-        atomicAdd(dst + 1, vi);
+        if (staged) {
+          atomicAdd(dst, vr);
+          atomicAdd(dst + 1, vi);
+        } else {
+          atomicAdd(reinterpret_cast<float2*>(dst), make_float2(vr, vi));  // one 8-byte global reduction
+        }
       }
     }
   }
@@ -611,12 +633,15 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
   const R beta = (R)P.beta;
   const R half = (R)0.5 * (R)w, inv = (R)1 / half;
   const int ncell = P.b1n * P.b2n;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // shared memory: [nw][SG*SG] complex subgrids, [nw][PB][2w] kernel weights,
-  // then (if it fits) a private copy of the band.  PB = points prepared per
-  // phase, the largest of 32/16/8 that fits.
-  const size_t sub_b = (size_t)nw * SG * SG * sizeof(cpx<R>);
+  // then (if it fits) a private copy of the band.  nw = the warps that own a
+  // subgrid (all of the CTA's when they fit), PB = points prepared per phase,
+  // the largest of 32/16/8 that fits.
   const size_t dyn_b = (size_t)c.dyn_cpx * sizeof(cpx<R>);
+  int nw = blockDim.x >> 5;
+  while (nw > 1 && (size_t)nw * (SG * SG * sizeof(cpx<R>) + 8 * 2 * w * sizeof(R)) + 16 > dyn_b) --nw;
+  const size_t sub_b = (size_t)nw * SG * SG * sizeof(cpx<R>);
   int PB = 32;
   while (PB > 8 && sub_b + (size_t)nw * PB * 2 * w * sizeof(R) > dyn_b) PB >>= 1;
   const size_t wt_b = ((size_t)nw * PB * 2 * w * sizeof(R) + 15) / 16 * 16;
@@ -631,7 +656,7 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
   }
   const int ra = lane % w, rb = lane / w;
   const int gw = g.rank * nw + warp, nwt = g.G * nw;
-  for (int it = gw; it < P.nitems; it += nwt) {
+  for (int it = warp < nw ? gw : P.nitems; it < P.nitems; it += nwt) {
     const int4 item = items[it];
     for (int i = lane; i < SG * SG; i += 32) sub[i] = cmk<R>(0, 0);
     for (int jb = item.x; jb < item.y; jb += PB) {
@@ -640,12 +665,7 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
       R cre_l = 0, cim_l = 0;
       int cell_l = 0;
       if (lane < PB && jl < item.y) {
-        const int e1 = off[jl + 1];
-        for (int e = off[jl]; e < e1; ++e) {
-          const cpx<R> q = contrib[ent[e]];
-          cre_l += q.x;
-          cim_l += q.y;
-        }
+        gather_contrib(ent, contrib, off[jl], off[jl + 1], cre_l, cim_l);
         const R xi1 = xu[jl], xi2 = xv[jl];
         const int l1 = (int)ceil(xi1 - half), l2 = (int)ceil(xi2 - half);
         R* wr = wtab + lane * 2 * w;

@@ -487,6 +487,11 @@ __device__ int select_from_range(LbCtx& c, const unsigned long long* sbk, const 
 // leader): batches of whole buckets (<= SMILI_KC elements) are sorted by
 // (t, index) and swept with the closed-form piecewise quadratic.  Writes the
 // CR_* results.
+// Bytes of dynamic shared memory the scan lays out (cand, hist, hist2, wtot,
+// dtm_s, t_s, Mm, st); the launch gives every CTA at least this much.
+constexpr size_t SMILI_CAUCHY_SMEM =
+    16 * SMILI_KC + 4 * SMILI_NBUCKET + 4 * 4096 +
+    8 * (SMILI_MAX_WARPS * 32 + 2 * SMILI_MAX_THREADS + 4 * SMILI_MAXM_DEV * SMILI_MAXM_DEV + 5 + 4 * SMILI_MAXM_DEV);
 __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak, int bnded,
                             const unsigned long long* sbk, const int* sbi, const int* ghist) {
   LbState& S = *c.S;
@@ -496,10 +501,10 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
   u128* cand = reinterpret_cast<u128*>(c.dyn);                        // SMILI_KC
   unsigned* hist = reinterpret_cast<unsigned*>(cand + SMILI_KC);      // NBUCKET (bucket counts)
   unsigned* hist2 = hist + SMILI_NBUCKET;                             // 4096 (fallback)
-  double* wtot = reinterpret_cast<double*>(hist2 + 4096);             // WARPS*32
-  double* dtm_s = wtot + SMILI_WARPS * 32;                            // THREADS
-  double* t_s = dtm_s + SMILI_THREADS;                                // THREADS
-  double* Mm = t_s + SMILI_THREADS;                                   // dense M (2col)^2
+  double* wtot = reinterpret_cast<double*>(hist2 + 4096);             // MAX_WARPS*32
+  double* dtm_s = wtot + SMILI_MAX_WARPS * 32;                        // MAX_THREADS
+  double* t_s = dtm_s + SMILI_MAX_THREADS;                            // MAX_THREADS
+  double* Mm = t_s + SMILI_MAX_THREADS;                               // dense M (2col)^2
   double* st = Mm + 4 * SMILI_MAXM_DEV * SMILI_MAXM_DEV;              // carried state
   // st: [0]=D [1]=tprev [2]=dtm_cur [3..] unused [5..5+2m)=P [..+2m)=Q
   __shared__ unsigned long long bnd_hi_s, bnd_lo_s;
@@ -617,7 +622,8 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
     pf.mark(PR_C_SORT);
     // ---------------- scan in chunks of THREADS ----------------
     bool finished = false;
-    for (int base = 0; base < cnt; base += SMILI_THREADS) {
+    const int T = blockDim.x;
+    for (int base = 0; base < cnt; base += T) {
       const int e = threadIdx.x;
       const int ge = base + e;
       const bool valid = ge < cnt;
@@ -673,13 +679,13 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
         const double pt = (e == 0) ? st[1] : t_s[e - 1];
         stop = pd < (te - pt);
       }
-      if (threadIdx.x == 0) e_star_s = SMILI_THREADS;
+      if (threadIdx.x == 0) e_star_s = T;
       __syncthreads();
       if (stop) atomicMin(&e_star_s, e);
       __syncthreads();
       const int es = e_star_s;
-      const int nvalid = min(SMILI_THREADS, cnt - base);
-      if (es < SMILI_THREADS) {
+      const int nvalid = min(T, cnt - base);
+      if (es < T) {
         // GCP inside the segment before element es: breakpoints up to es-1 fixed
         if ((es == 0 && threadIdx.x == 0) || (es > 0 && e == es - 1)) {
           double Pf[2 * SMILI_MAXM_DEV], Cf[2 * SMILI_MAXM_DEV];
@@ -793,7 +799,7 @@ __device__ int lb_cauchy(LbCtx& c) {
     double py[SMILI_MAXM_DEV], ps[SMILI_MAXM_DEV];
 #pragma unroll
     for (int j = 0; j < SMILI_MAXM_DEV; ++j) py[j] = ps[j] = 0.0;
-    for (int i = c.g->rank * SMILI_THREADS + threadIdx.x; i < 2 * SMILI_NBUCKET; i += c.g->G * SMILI_THREADS)
+    for (int i = c.g->rank * blockDim.x + threadIdx.x; i < 2 * SMILI_NBUCKET; i += c.g->G * blockDim.x)
       ghist[i] = 0;
     for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
       const double neggi = -c.gv[i];

@@ -290,12 +290,12 @@ __device__ bool movie_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
 }
 
 template <typename R>
-__global__ void __launch_bounds__(SMILI_THREADS, sizeof(R) == 4 ? 3 : 2) smili_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(Shape<R>::threads, Shape<R>::min_blocks) smili_batch_kernel(BatchArgs a) {
   extern __shared__ __align__(16) char dyn[];
   __shared__ LbState S;
   __shared__ double red[SMILI_REDK];
   __shared__ unsigned char ops[SMILI_REDK];
-  __shared__ double scratch[SMILI_WARPS * SMILI_REDK];
+  __shared__ double scratch[Shape<R>::warps * SMILI_REDK];
   __shared__ int prob_s;
   const int grp = blockIdx.x / a.G, rank = blockIdx.x % a.G;
   Prof prof;
@@ -518,6 +518,15 @@ std::vector<double> deconv_factors(int N, int nf, int w, double beta) {
   return out;
 }
 
+// Dynamic shared memory per CTA: the FFT/spread staging buffers, at least
+// 48 KB, and never less than the Cauchy scan's layout.
+template <typename R>
+size_t dyn_smem_bytes() {
+  size_t b = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
+  b = std::max(b, (SMILI_CAUCHY_SMEM + 1023) / 1024 * 1024);
+  return b;
+}
+
 struct Arena {
   size_t bytes = 0;
   int64_t take(size_t nbytes) {
@@ -707,13 +716,13 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.b2s = (int)mn2;
     d.b2n = (int)(mx2 - mn2 + 1);
   }
-  // spreading tile: 16 x 16 when its warp subgrids (8 warps of (16 + w - 1)^2
-  // complex values) and the smallest weight table fit the dynamic shared
-  // memory of the launch, else 8 x 8
+  // spreading tile: 16 x 16 when its warp subgrids (one (16 + w - 1)^2
+  // complex subgrid per warp) and the smallest weight table fit the dynamic
+  // shared memory of the launch, else 8 x 8
   {
-    const size_t dyn = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
-    const size_t sg = 16 + w - 1;
-    if (bin == 16 && 8 * sg * sg * sizeof(cpx<R>) + 8 * 8 * 2 * w * sizeof(R) + 16 > dyn) bin = 8;
+    const size_t dyn = (size_t)SMILI_DYN_CPX * sizeof(cpx<R>);
+    const size_t sg = 16 + w - 1, nw = Shape<R>::warps;
+    if (bin == 16 && nw * sg * sg * sizeof(cpx<R>) + nw * 8 * 2 * w * sizeof(R) + 16 > dyn) bin = 8;
     if (bin != 16) bin = 8;
   }
   d.bin = bin;
@@ -991,7 +1000,7 @@ int launch_batch(smili_batch* b, int mode, float* ms) {
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventRecord(e0, b->stream));
   }
-  CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(b->G * b->ngroups), dim3(SMILI_THREADS), args,
+  CUDA_TRY(cudaLaunchCooperativeKernel(fn, dim3(b->G * b->ngroups), dim3(Shape<R>::threads), args,
                                        b->dyn_bytes, b->stream));
   if (ms) {
     CUDA_TRY(cudaEventRecord(e1, b->stream));
@@ -1061,9 +1070,9 @@ int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smi
   }
   // launch geometry: co-resident CTAs split into groups
   // FFT/spread staging (SMILI_DYN_CPX complex values) and the Cauchy scan's
-  // batch buffers (about 47 KB) share the dynamic region: 96 KB in FP64 (two
-  // CTAs per SM), 48 KB in FP32 (three CTAs per SM)
-  b->dyn_bytes = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
+  // batch buffers share the dynamic region: 96 KB in FP64 (two CTAs per SM),
+  // 48 KB in FP32 (three CTAs per SM)
+  b->dyn_bytes = dyn_smem_bytes<R>();
   const void* fn = (const void*)smili_batch_kernel<R>;
   auto cleanup = [&](int rc) {
     smili_batch_destroy(b);
@@ -1072,14 +1081,15 @@ int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smi
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_bytes) != cudaSuccess)
     return cleanup(fail(SMILI_ERR_CUDA, "cannot set dynamic shared memory size"));
   int occ = 0, nsm = 0, coop = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, SMILI_THREADS, b->dyn_bytes));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, Shape<R>::threads, b->dyn_bytes));
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
   CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
   if (!coop || occ < 1) return cleanup(fail(SMILI_ERR_CUDA, "cooperative launch unavailable"));
   const int maxres = occ * nsm;
   int G = opt && opt->ctas_per_problem > 0 ? opt->ctas_per_problem : 0;
   if (G <= 0) {
-    G = std::max(1, std::min(maxres, (maxn + 1023) / 1024));
+    const int per_cta = 4 * Shape<R>::threads;  // about four pixels per thread
+    G = std::max(1, std::min(maxres, (maxn + per_cta - 1) / per_cta));
     if (nprob > 1) G = std::max(1, std::min(G, maxres / nprob));
   }
   G = std::min(G, maxres);
@@ -1780,8 +1790,8 @@ int noalloc_scratch(int device, char** out) {
     CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     if (!p || (reinterpret_cast<uintptr_t>(p) & 255u))
       return fail(SMILI_ERR_CUDA, "scratch symbol address is null or not 256-byte aligned");
-    const size_t dyn64 = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<double>), (size_t)48 * 1024);
-    const size_t dyn32 = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<float>), (size_t)48 * 1024);
+    const size_t dyn64 = dyn_smem_bytes<double>();
+    const size_t dyn32 = dyn_smem_bytes<float>();
     CUDA_TRY(cudaFuncSetAttribute((const void*)smili_batch_kernel<double>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn64));
     CUDA_TRY(cudaFuncSetAttribute((const void*)smili_batch_kernel<float>,
@@ -1822,10 +1832,10 @@ int calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_
   b.device = device;
   b.kind = PK_FG;
   b.descs.push_back(hp.d);
-  b.dyn_bytes = std::max((size_t)SMILI_DYN_CPX * sizeof(cpx<R>), (size_t)48 * 1024);
+  b.dyn_bytes = dyn_smem_bytes<R>();
   const void* fn = (const void*)smili_batch_kernel<R>;
   int occ = 0, nsm = 0, coop = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, SMILI_THREADS, b.dyn_bytes));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, Shape<R>::threads, b.dyn_bytes));
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
   CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
   if (!coop || occ < 1) return fail(SMILI_ERR_CUDA, "cooperative launch unavailable");

@@ -220,22 +220,27 @@ def test_survey_batch_mixed_sizes(lib):
 
 def test_spread_bin16_equals_bin8(oracle, closure40, lib):
     """16-cell spreading tiles give the same evaluation as 8-cell tiles (and
-    as the oracle); the autotuner returns one of its candidates."""
+    as the oracle); the autotuner returns one of its candidates.  FP64 at
+    nufft_eps 1e-6 (kernel width 7): eight warp subgrids of 22 x 22 complex
+    values and their weight tables (about 69 KB) fit the 96 KB of staging,
+    so the 16-cell tiles are really used."""
     from smili_b200 import autotune
-    from smili_b200.fortlib import fftim2d
     kw = make_kw(closure40)
     x = np.asarray(kw["iin"]) * np.random.default_rng(2).uniform(0.5, 1.5, np.size(kw["iin"]))
     prob = lib.Problem(dict(kw, iin=x))
     out = []
     for b in (8, 16):
-        bt = lib.Batch([prob], niter=1, options=lib.make_options(64, 1e-12, spread_bin=b))
+        bt = lib.Batch([prob], niter=1, options=lib.make_options(64, 1e-6, spread_bin=b))
         bt.run(fg_only=1)
         _, t, g, _ = bt.fetch(0)
         bt.close()
         out.append((t["cost"], g))
+    # the same sums in another order: FP64 roundoff only
     assert abs(out[1][0] - out[0][0]) <= 1e-12 * abs(out[0][0])
     assert np.max(np.abs(out[1][1] - out[0][1])) <= 1e-10 * np.max(np.abs(out[0][1]))
+    # against the exact transform: the NUFFT tolerance
     t_o, g_o = oracle.calc_cost(kw, x, eps=0.0)
-    assert abs(out[1][0] - t_o["cost"]) <= 1e-9 * abs(t_o["cost"])
+    assert abs(out[1][0] - t_o["cost"]) <= 1e-5 * abs(t_o["cost"])
+    assert np.max(np.abs(out[1][1] - g_o)) <= 1e-4 * np.max(np.abs(g_o))
     r = autotune.tune([kw] * 4, 32, niter=3, repeats=1, cands=[(1, 8), (2, 16)])
     assert (r["ctas_per_problem"], r["spread_bin"]) in [(1, 8), (2, 16)] and len(r["table"]) == 2
