@@ -71,6 +71,10 @@ typedef struct {
   int spread_bin;       /* spreading tile side in fine-grid cells: 8 or 16; 0 -> 8.  A
                            16-cell tile whose subgrids do not fit in shared memory
                            falls back to 8 */
+  int transform;        /* fine-grid passes of the NUFFT: 0 -> automatic, 1 -> FFTs,
+                           2 -> dense products with the twiddle matrices (used only
+                           where the data's band is at most 64 x 64 fine-grid cells;
+                           otherwise FFTs) */
 } smili_options;
 
 typedef struct {

@@ -54,7 +54,8 @@ class ImagingArgs(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("nufft_eps", C.c_double), ("ctas_per_problem", C.c_int),
-                ("device", C.c_int), ("stream", C.c_void_p), ("spread_bin", C.c_int)]
+                ("device", C.c_int), ("stream", C.c_void_p), ("spread_bin", C.c_int),
+                ("transform", C.c_int)]
 
 
 class ImagingArgs3D(C.Structure):
@@ -151,9 +152,11 @@ def dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def make_options(precision=64, nufft_eps=0.0, ctas_per_problem=0, device=0, stream=None, spread_bin=0):
+def make_options(precision=64, nufft_eps=0.0, ctas_per_problem=0, device=0, stream=None, spread_bin=0,
+                 transform=0):
     o = Options()
     o.spread_bin = int(spread_bin)
+    o.transform = int(transform)
     o.precision = int(precision)
     o.nufft_eps = float(nufft_eps)
     o.ctas_per_problem = int(ctas_per_problem)

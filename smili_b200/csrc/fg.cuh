@@ -82,12 +82,229 @@ struct KSumF {
 };
 
 // ---------------------------------------------------------------------------
+// Band passes as dense products (P.dft): with the twiddle matrices
+//   Ex[b][ix] = exp(+2 pi i (ix - nx/2)(b1s + b) / nf1)   [b1n][nx]
+//   Ey[r][iy] = exp(+2 pi i (iy - ny/2)(b2s + r) / nf2)   [b2n][ny]
+// the four FFT passes of the band-pruned NUFFT are
+//   F1  tmpA[iy][b]  = sum_ix U[iy][ix] Ex[b][ix],  U = x dc1[ix] dc2[iy]
+//   F2  bandA[r][b]  = sum_iy Ey[r][iy] tmpA[iy][b]
+//   F6  tmpC[r][ix]  = sum_b  bandC[r][b] Ex[b][ix]
+//   F7  gchi[iy][ix] = Re sum_r Ey[r][iy] tmpC[r][ix]  * dc1[ix] dc2[iy]
+// (the same twiddles the radix passes apply, exp periodic in nf).  Used
+// for bands of at most 64 x 64 cells, where each pass is a few million
+// multiply-adds that run as register-tiled loops.
+// ---------------------------------------------------------------------------
+constexpr int DFT_NB = 64;  // largest band side on this path
+constexpr int DFT_KC = 32;  // image columns per staged chunk in F1
+
+// F1 on the DFT path; also writes the dense image grid and the moments.
+// Threads: 16 column lanes x (T/16) row lanes; each thread accumulates 2 rows
+// x 4 band columns (b = lane, lane + 16, ...).  Row blocks of 2 T/16 rows go
+// to the group's CTAs in turn; per block the image and Ex are staged in
+// chunks of DFT_KC columns (rows padded by one element against bank
+// conflicts).
+template <typename R>
+__device__ void dft_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
+  const ProbDesc& P = *c.P;
+  const double* x = at<double>(c.base, P.o_x);
+  const int* inv = at<int>(c.base, P.o_inv);
+  double* xg = at<double>(c.base, P.o_xg);
+  const double* dc1 = at<double>(c.base, P.o_dc1);
+  const double* dc2 = at<double>(c.base, P.o_dc2);
+  const cpx<R>* Ex = at<cpx<R>>(c.base, P.o_ex);
+  cpx<R>* tmpA = at<cpx<R>>(c.base, P.o_tmpA);
+  cpx<R>* bandC = at<cpx<R>>(c.base, P.o_bandC);
+  const int nx = P.nx, ny = P.ny, nb = P.b1n;
+  const int T = blockDim.x, tc = threadIdx.x & 15, tr = threadIdx.x >> 4;
+  const int RB = 2 * (T >> 4);  // rows per block
+  const int KP = DFT_KC + 1;
+  R* Us = reinterpret_cast<R*>(c.sbuf);                                             // [RB][KP]
+  cpx<R>* Es = reinterpret_cast<cpx<R>*>(c.sbuf) + ((size_t)RB * KP * sizeof(R) + sizeof(cpx<R>) - 1) / sizeof(cpx<R>);  // [64][KP]
+  for (int i = g.rank * T + threadIdx.x; i < P.b2n * P.b1n; i += g.G * T) bandC[i] = cmk<R>(0, 0);
+  const bool need_mom = P.has_tfd || P.has_cen || P.has_sm;
+  for (int y0 = g.rank * RB; y0 < ny; y0 += g.G * RB) {
+    cpx<R> acc[2][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[a][q] = cmk<R>(0, 0);
+    for (int k0 = 0; k0 < nx; k0 += DFT_KC) {
+      for (int i = threadIdx.x; i < RB * DFT_KC; i += T) {
+        const int rr = i / DFT_KC, kk = i - rr * DFT_KC, iy = y0 + rr, ix = k0 + kk;
+        R u = 0;
+        if (iy < ny && ix < nx) {
+          const int pv = inv[iy * nx + ix];
+          const double val = pv >= 0 ? x[pv] : 0.0;
+          xg[(size_t)iy * nx + ix] = val;
+          u = (R)(val * dc1[ix] * dc2[iy]);
+          if (need_mom && pv >= 0) {
+            const double fx = ix + 1, fy = iy + 1;  // 1-based pixel numbers as the reference
+            mom[0] += val;
+            mom[1] += fabs(val);
+            mom[2] += val * fx;
+            mom[3] += val * fy;
+            mom[4] += val * fx * fx;
+            mom[5] += val * fy * fy;
+            mom[6] += val * fx * fy;
+            if (P.has_cen) {
+              const double Ip = fabs(P.cen_alpha - 1) < 1e-10 ? smabs(val) : pow(smabs(val), P.cen_alpha);
+              mom[7] += Ip * (fx - P.nxref);
+              mom[8] += Ip * (fy - P.nyref);
+              mom[9] += Ip;
+            }
+          }
+        }
+        Us[rr * KP + kk] = u;
+      }
+      for (int i = threadIdx.x; i < DFT_NB * DFT_KC; i += T) {
+        const int b = i / DFT_KC, kk = i - b * DFT_KC, ix = k0 + kk;
+        Es[b * KP + kk] = (b < nb && ix < nx) ? Ex[(size_t)b * nx + ix] : cmk<R>(0, 0);
+      }
+      __syncthreads();
+      const R* u0 = Us + (2 * tr) * KP;
+#pragma unroll 4
+      for (int kk = 0; kk < DFT_KC; ++kk) {
+        const R ua = u0[kk], ub = u0[KP + kk];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const cpx<R> e = Es[(tc + 16 * q) * KP + kk];
+          acc[0][q].x += ua * e.x;
+          acc[0][q].y += ua * e.y;
+          acc[1][q].x += ub * e.x;
+          acc[1][q].y += ub * e.y;
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      const int iy = y0 + 2 * tr + a;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int b = tc + 16 * q;
+        if (iy < ny && b < nb) tmpA[(size_t)iy * nb + b] = acc[a][q];
+      }
+    }
+  }
+}
+
+// F2 on the DFT path: one band cell per thread and pass; tmpA and Ey staged
+// in chunks of DFT_KC rows.
+template <typename R>
+__device__ void dft_t2_cols(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* Ey = at<cpx<R>>(c.base, P.o_ey);
+  const cpx<R>* tmpA = at<cpx<R>>(c.base, P.o_tmpA);
+  cpx<R>* bandA = at<cpx<R>>(c.base, P.o_bandA);
+  const int ny = P.ny, nb = P.b1n, nr = P.b2n, ncell = nb * nr;
+  const int T = blockDim.x, KP = DFT_KC + 1;
+  cpx<R>* As = c.sbuf;                   // [DFT_KC][nb]
+  cpx<R>* Ys = c.sbuf + DFT_KC * DFT_NB;  // [nr][KP]
+  for (int o0 = g.rank * T; o0 < ncell; o0 += g.G * T) {
+    const int o = o0 + threadIdx.x, r = o / nb, b = o - r * nb;
+    cpx<R> acc = cmk<R>(0, 0);
+    for (int k0 = 0; k0 < ny; k0 += DFT_KC) {
+      for (int i = threadIdx.x; i < DFT_KC * nb; i += T) {
+        const int kk = i / nb, bb = i - kk * nb;
+        As[i] = k0 + kk < ny ? tmpA[(size_t)(k0 + kk) * nb + bb] : cmk<R>(0, 0);
+      }
+      for (int i = threadIdx.x; i < nr * DFT_KC; i += T) {
+        const int rr = i / DFT_KC, kk = i - rr * DFT_KC;
+        Ys[rr * KP + kk] = k0 + kk < ny ? Ey[(size_t)rr * ny + k0 + kk] : cmk<R>(0, 0);
+      }
+      __syncthreads();
+      if (o < ncell) {
+#pragma unroll 4
+        for (int kk = 0; kk < DFT_KC; ++kk) {
+          const cpx<R> e = Ys[r * KP + kk], t = As[kk * nb + b];
+          acc.x += e.x * t.x - e.y * t.y;
+          acc.y += e.x * t.y + e.y * t.x;
+        }
+      }
+      __syncthreads();
+    }
+    if (o < ncell) bandA[o] = acc;
+  }
+}
+
+// F6 on the DFT path: bandC staged whole; a thread takes one image column
+// and up to 8 band rows, streaming its column of Ex.
+template <typename R>
+__device__ void dft_t1_rows(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* Ex = at<cpx<R>>(c.base, P.o_ex);
+  const cpx<R>* bandC = at<cpx<R>>(c.base, P.o_bandC);
+  cpx<R>* tmpC = at<cpx<R>>(c.base, P.o_tmpC);
+  const int nx = P.nx, nb = P.b1n, nr = P.b2n;
+  const int T = blockDim.x;
+  cpx<R>* Bs = c.sbuf;  // [nr][nb]
+  for (int i = threadIdx.x; i < nr * nb; i += T) Bs[i] = bandC[i];
+  __syncthreads();
+  const int ngrp = (nr + 7) >> 3, items = nx * ngrp;
+  for (int it = g.rank * T + threadIdx.x; it < items; it += g.G * T) {
+    const int rg = it / nx, ix = it - rg * nx, r0 = 8 * rg;
+    cpx<R> acc[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j] = cmk<R>(0, 0);
+    for (int b = 0; b < nb; ++b) {
+      const cpx<R> e = Ex[(size_t)b * nx + ix];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (r0 + j < nr) {
+          const cpx<R> v = Bs[(r0 + j) * nb + b];
+          acc[j].x += v.x * e.x - v.y * e.y;
+          acc[j].y += v.x * e.y + v.y * e.x;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (r0 + j < nr) tmpC[(size_t)(r0 + j) * nx + ix] = acc[j];
+  }
+  __syncthreads();
+}
+
+// F7 on the DFT path: a thread takes one image column and 4 image rows.
+template <typename R>
+__device__ void dft_t1_cols(FgCtx<R>& c, const GroupCtx& g) {
+  const ProbDesc& P = *c.P;
+  const cpx<R>* Ey = at<cpx<R>>(c.base, P.o_ey);
+  const cpx<R>* tmpC = at<cpx<R>>(c.base, P.o_tmpC);
+  const double* dc1 = at<double>(c.base, P.o_dc1);
+  const double* dc2 = at<double>(c.base, P.o_dc2);
+  double* gchi = at<double>(c.base, P.o_gchi);
+  const int nx = P.nx, ny = P.ny, nr = P.b2n;
+  const int T = blockDim.x, ngrp = (ny + 3) >> 2, items = nx * ngrp;
+  for (int it = g.rank * T + threadIdx.x; it < items; it += g.G * T) {
+    const int yg = it / nx, ix = it - yg * nx, y0 = 4 * yg;
+    R acc[4] = {0, 0, 0, 0};
+    for (int r = 0; r < nr; ++r) {
+      const cpx<R> t = tmpC[(size_t)r * nx + ix];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (y0 + j < ny) {
+          const cpx<R> e = Ey[(size_t)r * ny + y0 + j];
+          acc[j] += e.x * t.x - e.y * t.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (y0 + j < ny) gchi[(size_t)(y0 + j) * nx + ix] = (double)acc[j] * dc1[ix] * dc2[y0 + j];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // F1: type-2 row pass.  Deconvolved image rows -> band columns of the
 // row-transformed fine grid (tmpA[iy][b], b < b1n).  Also zeroes bandC.
 // Optionally accumulates image moments for the global regularizers.
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
+  if (c.P->dft) {
+    dft_t2_rows(c, g, mom);
+    return;
+  }
   const ProbDesc& P = *c.P;
   const double* x = at<double>(c.base, P.o_x);
   const int* inv = at<int>(c.base, P.o_inv);
@@ -145,6 +362,10 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ void fg_t2_cols(FgCtx<R>& c, const GroupCtx& g) {
+  if (c.P->dft) {
+    dft_t2_cols(c, g);
+    return;
+  }
   const ProbDesc& P = *c.P;
   const cpx<R>* tw2 = at<cpx<R>>(c.base, P.o_tw2);
   const cpx<R>* tmpA = at<cpx<R>>(c.base, P.o_tmpA);
@@ -732,6 +953,10 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ void fg_t1_rows(FgCtx<R>& c, const GroupCtx& g) {
+  if (c.P->dft) {
+    dft_t1_rows(c, g);
+    return;
+  }
   const ProbDesc& P = *c.P;
   const cpx<R>* tw1 = at<cpx<R>>(c.base, P.o_tw1);
   const cpx<R>* bandC = at<cpx<R>>(c.base, P.o_bandC);
@@ -762,6 +987,10 @@ __device__ void fg_t1_rows(FgCtx<R>& c, const GroupCtx& g) {
 // ---------------------------------------------------------------------------
 template <typename R>
 __device__ void fg_t1_cols(FgCtx<R>& c, const GroupCtx& g) {
+  if (c.P->dft) {
+    dft_t1_cols(c, g);
+    return;
+  }
   const ProbDesc& P = *c.P;
   const cpx<R>* tw2 = at<cpx<R>>(c.base, P.o_tw2);
   const cpx<R>* tmpC = at<cpx<R>>(c.base, P.o_tmpC);

@@ -42,6 +42,8 @@ struct ProbDesc {
   int windowed;            // 1 when the pixel set is not the full nx*ny grid
   int nitems;              // spreading work items (<= 128 points of one bin x bin tile)
   int bin;                 // spreading bin side in fine-grid cells (8 or 16)
+  int dft;                 // 1: the four band passes as dense products with the
+                           // twiddle matrices o_ex / o_ey instead of FFTs
   // movies (dynamic imaging): nframes >= 1 on a movie's descriptor (0 for a
   // 2D problem), whose vectors hold npix = frame_npix * nframes values; each
   // frame is a 2D descriptor (o_frames) whose x / g / d point into them
@@ -59,6 +61,7 @@ struct ProbDesc {
   // byte offsets in the arena (0 = absent)
   int64_t o_x0, o_xidx, o_yidx, o_inv;
   int64_t o_xg;                         // dense image grid [ny][nx] (double), written by F1
+  int64_t o_ex, o_ey;                   // twiddle matrices [b1n][nx], [b2n][ny] (cpx<R>) when dft
   int64_t o_l1w, o_tvw, o_tsvw, o_klw, o_gsw;
   int64_t o_dc1, o_dc2, o_tw1, o_tw2;   // deconvolution factors, twiddle tables
   int64_t o_u, o_v;                     // fine-grid coordinates xi = u n / 2pi (R)

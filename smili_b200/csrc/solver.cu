@@ -560,7 +560,8 @@ enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4, PK_MODEL = 5
 template <typename R>
 int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, int m, double factr,
                  double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override,
-                 const double* c_re, const double* c_im, double wtotal_override = 0.0, int bin = 8) {
+                 const double* c_re, const double* c_im, double wtotal_override = 0.0, int bin = 8,
+                 int transform = 0) {
   ProbDesc& d = hp.d;
   std::memset(&d, 0, sizeof(d));
   const int N = a.npix, nx = a.nx, ny = a.ny, nuv = a.nuv;
@@ -726,6 +727,18 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     if (bin != 16) bin = 8;
   }
   d.bin = bin;
+  // band passes: dense products with the twiddle matrices when the band is
+  // narrow (at most 64 x 64 cells, 2048 in all) and their multiply-adds
+  // (2 nx ny b1n + 4 b1n ny b2n per direction, real and complex halves) come
+  // to less than twice the radix passes' flops; they run as register-tiled
+  // loops, the FFTs as latency-bound shared-memory sweeps
+  {
+    const bool fits = d.b1n <= 64 && d.b2n <= 64 && d.b1n * d.b2n <= 2048;
+    const double lg1 = std::log2((double)d.nf1), lg2 = std::log2((double)d.nf2);
+    const double dft_fl = 2.0 * nx * ny * (d.b1n + d.b2n) + 8.0 * d.b1n * d.b2n * (nx + ny);
+    const double fft_fl = 5.0 * ((double)(ny + d.b2n) * d.nf1 * lg1 + (double)(d.b1n + nx) * d.nf2 * lg2);
+    d.dft = fits && (transform == 2 || (transform == 0 && dft_fl < 2.0 * fft_fl));
+  }
   // sort the uv points by bin x bin tiles of the band (spreading subproblems
   // and locality); remap indices.  Band-relative cells are computed exactly as the
   // kernels do: imod(ceil(xi - w/2) - start, nf).
@@ -870,6 +883,10 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.o_dc2 = ar.take(sizeof(double) * ny);
   d.o_tw1 = ar.take(C * d.nf1);
   d.o_tw2 = ar.take(C * d.nf2);
+  if (d.dft) {
+    d.o_ex = ar.take(C * (size_t)d.b1n * nx);
+    d.o_ey = ar.take(C * (size_t)d.b2n * ny);
+  }
   d.o_u = ar.take(sizeof(R) * nuv);
   d.o_v = ar.take(sizeof(R) * nuv);
   d.o_dre = ar.take(sizeof(R) * dre.size());
@@ -926,6 +943,23 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   hp.put(d.o_dc2, dc2);
   hp.put(d.o_tw1, twiddles(d.nf1));
   hp.put(d.o_tw2, twiddles(d.nf2));
+  if (d.dft) {
+    // E[b][i] = tw[((i - n_img / 2) (bs + b)) mod nf]: the twiddle each FFT
+    // pass applies between image index i and band index b
+    auto emat = [&](int nb, int bs, int nimg, int nf) {
+      const std::vector<cpx<R>> tw = twiddles(nf);
+      std::vector<cpx<R>> e((size_t)nb * nimg);
+      for (int b = 0; b < nb; ++b)
+        for (int i = 0; i < nimg; ++i) {
+          long k = ((long)(i - nimg / 2) * (long)(bs + b)) % nf;
+          if (k < 0) k += nf;
+          e[(size_t)b * nimg + i] = tw[k];
+        }
+      return e;
+    };
+    hp.put(d.o_ex, emat(d.b1n, d.b1s, nx, d.nf1));
+    hp.put(d.o_ey, emat(d.b2n, d.b2s, ny, d.nf2));
+  }
   hp.put(d.o_u, su);
   hp.put(d.o_v, sv);
   hp.put(d.o_dre, dre);
@@ -1039,7 +1073,7 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   for (int p = 0; p < nprob; ++p) {
     const int rc = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ar,
                                    hps[p], x_over ? x_over[p] : nullptr, c_re, c_im, 0.0,
-                                   opt && opt->spread_bin ? opt->spread_bin : 8);
+                                   opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
     if (rc != SMILI_OK) {
       delete b;
       return rc;
@@ -1156,7 +1190,8 @@ int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smi
 // movie's vectors.
 template <typename R>
 int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, int m, double factr,
-               double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override, int spread_bin) {
+               double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override, int spread_bin,
+               int transform) {
   const int N = a.npix, Nz = a.nz, nuv = a.nuv;
   if (N < 1 || Nz < 1 || nuv < 0 || a.nx < 1 || a.ny < 1 || (long)N * Nz > 0x7fffffffL)
     return fail(SMILI_ERR_ARG, "invalid movie sizes");
@@ -1381,7 +1416,7 @@ int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, i
     fa.wca = a.wca;
     fa.inormfactr = a.inormfactr;
     if ((rc = pack_problem<R>(fa, PK_FRAME, 0, nonneg, m, factr, pgtol, eps, ar, fh[z], nullptr, nullptr, nullptr,
-                              wtotal, spread_bin)) != SMILI_OK)
+                              wtotal, spread_bin, transform)) != SMILI_OK)
       return rc;
     ProbDesc& F = fh[z].d;
     F.o_x = d.o_x + (int64_t)sizeof(double) * z * N;
@@ -1418,7 +1453,7 @@ int create_movie(const smili_imaging3d_args* a, int kind, int niter, int nonneg,
   Arena ar;
   std::vector<HostProb> hps(1);
   const int rc = pack_movie<R>(*a, kind, niter, nonneg, m, factr, pgtol, eps, ar, hps[0], x_over,
-                               opt && opt->spread_bin ? opt->spread_bin : 8);
+                               opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
   if (rc != SMILI_OK) {
     delete b;
     return rc;
@@ -1449,7 +1484,7 @@ int create_model(const smili_imaging_args& a, const double* x, const smili_optio
   Arena ar;
   std::vector<HostProb> hps(1);
   const int rc = pack_problem<R>(b0, PK_MODEL, 0, 0, 5, 1e1, 0.0, eps, ar, hps[0], x, nullptr, nullptr, w,
-                                 opt && opt->spread_bin ? opt->spread_bin : 8);
+                                 opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
   if (rc != SMILI_OK) {
     delete b;
     return rc;

@@ -16,29 +16,30 @@ import numpy as np
 from .. import _lib
 
 
-def nufft_fwd_real(u, v, i2d, precision=64, nufft_eps=0.0, device=0):
-    """Type-2 NUFFT of the (nx, ny) Fortran-order image ``i2d``; returns (Vreal, Vimag)."""
+def nufft_fwd_real(u, v, i2d, precision=64, nufft_eps=0.0, device=0, transform=0):
+    """Type-2 NUFFT of the (nx, ny) Fortran-order image ``i2d``; returns (Vreal, Vimag).
+    ``transform``: 0 automatic, 1 FFT passes, 2 dense twiddle products (narrow bands)."""
     u = np.ascontiguousarray(u, dtype=np.float64)
     v = np.ascontiguousarray(v, dtype=np.float64)
     img = np.asarray(i2d, dtype=np.float64)
     nx, ny = img.shape
     flat = np.ascontiguousarray(img.reshape(-1, order="F"))
     vr, vi = np.zeros(u.size), np.zeros(u.size)
-    opt = _lib.make_options(precision, nufft_eps, 0, device)
+    opt = _lib.make_options(precision, nufft_eps, 0, device, transform=transform)
     _lib.check(_lib.lib().smili_nufft_fwd_real(u.size, _lib.dptr(u), _lib.dptr(v), nx, ny,
                                                _lib.dptr(flat), C.byref(opt), _lib.dptr(vr),
                                                _lib.dptr(vi)))
     return vr, vi
 
 
-def nufft_adj_real1d(u, v, vreal, vimag, nx, ny, precision=64, nufft_eps=0.0, device=0):
+def nufft_adj_real1d(u, v, vreal, vimag, nx, ny, precision=64, nufft_eps=0.0, device=0, transform=0):
     """Real part of the type-1 NUFFT of Vreal + i Vimag, as an Nx*Ny vector."""
     u = np.ascontiguousarray(u, dtype=np.float64)
     v = np.ascontiguousarray(v, dtype=np.float64)
     vr = np.ascontiguousarray(vreal, dtype=np.float64)
     vi = np.ascontiguousarray(vimag, dtype=np.float64)
     out = np.zeros(int(nx) * int(ny))
-    opt = _lib.make_options(precision, nufft_eps, 0, device)
+    opt = _lib.make_options(precision, nufft_eps, 0, device, transform=transform)
     _lib.check(_lib.lib().smili_nufft_adj_real1d(u.size, _lib.dptr(u), _lib.dptr(v), _lib.dptr(vr),
                                                  _lib.dptr(vi), int(nx), int(ny), C.byref(opt),
                                                  _lib.dptr(out)))

@@ -50,8 +50,9 @@ def from_grid(kw, img):
                                 * float(kw["inormfactr"]), dtype=np.float64)
 
 
-def dirty_images(kws, device=0, chunk=1024):
-    """Normalised dirty images (N, ny, nx): -grad chi2_fcv at x = 0, max |.| 1."""
+def dirty_images(kws, device=0, chunk=1024, kernel_ms=None):
+    """Normalised dirty images (N, ny, nx): -grad chi2_fcv at x = 0, max |.| 1.
+    ``kernel_ms`` (a list) receives the device time of each evaluation launch."""
     out = []
     for c0 in range(0, len(kws), chunk):
         part = kws[c0:c0 + chunk]
@@ -64,7 +65,9 @@ def dirty_images(kws, device=0, chunk=1024):
                 k[name] = -1.0
             probs.append(k)
         b = _lib.Batch(probs, niter=0, options=_lib.make_options(64, 1e-6, device=device))
-        b.run(fg_only=1)
+        ms = b.run(fg_only=1)
+        if kernel_ms is not None:
+            kernel_ms.append(ms)
         for p, kw in enumerate(part):
             g = b.fetch(p)[2]
             d = -to_grid(kw, g)

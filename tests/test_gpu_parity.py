@@ -51,6 +51,66 @@ def test_nufft_adj_matches_dft(oracle, nx, ny):
     assert _rel(got, ex) < 1e-10
 
 
+def _band(u, nf, eps):
+    """Band width in fine-grid cells that the library computes for these
+    coordinates (kernel width w = ceil(log10(10 / eps)))."""
+    w = int(np.ceil(np.log10(10.0 / eps)))
+    l = np.ceil(np.asarray(u) * nf / (2 * np.pi) - 0.5 * w)
+    return int(l.max() - l.min() + w)
+
+
+@pytest.mark.parametrize("transform", [1, 2])
+@pytest.mark.parametrize("nx,ny", [(32, 32), (40, 24), (96, 96)])
+def test_nufft_transform_paths_match_dft(oracle, nx, ny, transform):
+    """Both fine-grid paths (radix passes, dense twiddle products) against
+    the exact transform, in both directions and precisions.  The points lie
+    in |u|, |v| < 0.4 rad/pixel, so the band is narrow enough for the dense
+    path (at most 64 x 64 cells, 2048 in all)."""
+    from smili_b200.fortlib import fftlib
+    rng = np.random.default_rng(nx + 7 * ny)
+    img = rng.standard_normal((ny, nx))
+    u, v = rng.uniform(-0.4, 0.4, 900), rng.uniform(-0.4, 0.4, 900)
+    nf1, nf2 = 2 * nx, 2 * ny  # next235even(2n) for these sizes
+    b1, b2 = _band(u, nf1, 1e-12), _band(v, nf2, 1e-12)
+    assert b1 <= 64 and b2 <= 64 and b1 * b2 <= 2048
+    ex = oracle.nufft2d2(u, v, img, 0)
+    vr, vi = fftlib.nufft_fwd_real(u, v, img.T, nufft_eps=1e-12, transform=transform)
+    assert _rel(vr + 1j * vi, ex) < 1e-10
+    vr, vi = fftlib.nufft_fwd_real(u, v, img.T, precision=32, nufft_eps=1e-6, transform=transform)
+    assert _rel(vr + 1j * vi, ex) < 2e-5
+    c = rng.standard_normal(u.size) + 1j * rng.standard_normal(u.size)
+    ex1 = oracle.nufft2d1(u, v, c, nx, ny, 0).real.reshape(-1)
+    got = fftlib.nufft_adj_real1d(u, v, c.real, c.imag, nx, ny, nufft_eps=1e-12, transform=transform)
+    assert _rel(got, ex1) < 1e-10
+    got = fftlib.nufft_adj_real1d(u, v, c.real, c.imag, nx, ny, precision=32, nufft_eps=1e-6,
+                                  transform=transform)
+    assert _rel(got, ex1) < 2e-5
+
+
+@pytest.mark.parametrize("prec,tol", [(64, 1e-12), (32, 1e-5)])
+def test_calc_cost_transform_paths_agree(oracle, closure40, lib, prec, tol):
+    """One evaluation of the closure-term problem through the radix passes
+    and through the dense twiddle products: the same objective and gradient
+    (FP64: roundoff; FP32: both within FP32 accuracy), and the oracle's."""
+    kw = make_kw(closure40)
+    nf = 2 * int(kw["nx"])
+    b1, b2 = _band(kw["u"], nf, 1e-6), _band(kw["v"], nf, 1e-6)
+    assert b1 <= 64 and b2 <= 64 and b1 * b2 <= 2048, (b1, b2)
+    x = np.asarray(kw["iin"]) * np.random.default_rng(4).uniform(0.5, 1.5, np.size(kw["iin"]))
+    prob = lib.Problem(dict(kw, iin=x))
+    out = []
+    for tr in (1, 2):
+        bt = lib.Batch([prob], niter=1, options=lib.make_options(prec, 1e-6, transform=tr))
+        bt.run(fg_only=1)
+        _, t, g, _ = bt.fetch(0)
+        bt.close()
+        out.append((t["cost"], g))
+    assert abs(out[1][0] - out[0][0]) <= tol * abs(out[0][0])
+    assert np.max(np.abs(out[1][1] - out[0][1])) <= 10 * tol * np.max(np.abs(out[0][1]))
+    t_o, g_o = oracle.calc_cost(kw, x, eps=0.0)
+    assert abs(out[1][0] - t_o["cost"]) <= 1e-5 * abs(t_o["cost"])
+
+
 def test_nufft_band_localised_points(oracle):
     """VLBI-like coverage: all points within a narrow band of the fine grid."""
     from smili_b200.fortlib import fftlib
