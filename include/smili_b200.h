@@ -190,6 +190,18 @@ int smili_calc_cost3d(const smili_imaging3d_args* a, const double* x, const smil
 int smili_model_terms(const smili_imaging_args* a, const double* x, const smili_options* opt, double* chisq,
                       double* grad, double* model_re, double* model_im, double* resid_re, double* resid_im);
 
+/* The non-redundant uv list of get_uvlist (smili/uvdata/uvtable/tools.py:
+ * 12-132), computed on the GPU.  u, v: the n uv points of all data terms
+ * stacked in the reference's order (fcv, amp, closure phases uv12 | uv23 |
+ * uv31, closure amplitudes uv1 | uv2 | uv3 | uv4, each block contiguous).
+ * A point with v < 0 counts as (-u, -v) with sign -1.  Out: *nuv distinct
+ * folded points in u_out, v_out (capacity n) in the order np.unique gives
+ * complex values (u, then v; -0 equals +0), each as first stacked; uvidx[n]
+ * = sign * (1 + position of the point in that list), in stack order.
+ * Device memory is allocated for the call and freed before it returns. */
+int smili_get_uvlist(int n, const double* u, const double* v, const smili_options* opt, int* nuv,
+                     double* u_out, double* v_out, int* uvidx);
+
 /* NUFFTs of the imaging path with the reference's conventions (sign "+",
  * modes -N/2..(N-1)/2 at pixels 1..N): fortlib.fftlib.nufft_fwd_real
  * (type 2, fftlib.f90:86-100) and nufft_adj_real1d (type 1, real part,

@@ -105,7 +105,7 @@ EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "sm
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
            "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile",
            "smili_batch_set_targets", "smili_calc_cost_noalloc", "smili_fftim3d_imaging",
-           "smili_calc_cost3d", "smili_model_terms"]
+           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist"]
 STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
           "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
           "c_gather", "c_sort", "c_scan", "c_rounds"]
@@ -128,6 +128,7 @@ def lib():
                                             C.c_double, vp, dp, dp, vp]
         L.smili_calc_cost3d.argtypes = [vp, dp, vp, dp, dp]
         L.smili_model_terms.argtypes = [vp, dp, vp, C.POINTER(C.c_double), dp, dp, dp, dp, dp]
+        L.smili_get_uvlist.argtypes = [C.c_int, dp, dp, vp, C.POINTER(C.c_int), dp, dp, C.POINTER(C.c_int)]
         L.smili_batch_create.argtypes = [C.c_int, C.POINTER(vp), ip, C.c_int, C.c_int, C.c_double,
                                          C.c_double, vp, C.POINTER(vp)]
         L.smili_batch_run.argtypes = [vp, C.c_int, C.POINTER(C.c_float)]

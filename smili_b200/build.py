@@ -16,7 +16,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 
 # output -> (main source, dependencies under csrc/, headers under include/)
 LIBS = {
-    "libsmili_b200.so": ("solver.cu", ["common.cuh", "fft.cuh", "fg.cuh", "lbfgsb.cuh", "layout.h"],
+    "libsmili_b200.so": ("solver.cu", ["common.cuh", "fft.cuh", "fg.cuh", "lbfgsb.cuh", "layout.h", "uvlist.cuh"],
                          ["smili_b200.h"]),
     "libsmili_unet.so": ("unet.cu", [], ["smili_unet.h"]),
 }

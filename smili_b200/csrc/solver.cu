@@ -1792,6 +1792,14 @@ int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const doub
 
 }  // extern "C"
 
+#include "uvlist.cuh"
+
+extern "C" int smili_get_uvlist(int n, const double* u, const double* v, const smili_options* opt, int* nuv,
+                                double* u_out, double* v_out, int* uvidx) {
+  return uvlist_run(n, u, v, opt ? opt->device : 0, opt ? static_cast<cudaStream_t>(opt->stream) : nullptr, nuv,
+                    u_out, v_out, uvidx);
+}
+
 // ===========================================================================
 // Allocation-free calc_cost (no reference counterpart)
 //

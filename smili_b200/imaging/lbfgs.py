@@ -68,9 +68,12 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
                     tsv_prior=None, kl_lambda=-1, kl_prior=None, gs_lambda=-1, gs_prior=None,
                     tfd_lambda=-1, tfd_tgterror=0.01, cen_lambda=-1, cen_alpha=3, sm_lambda=-1,
                     sm_maj=0., sm_min=0., sm_phi=0., pulse_fwhm=-1, niter=1000, nonneg=True,
-                    nprint=500, totalflux=None, inorm=1., istokes=0, ifreq=0, verbose=False):
+                    nprint=500, totalflux=None, inorm=1., istokes=0, ifreq=0, verbose=False,
+                    uvlist_device=None):
     """Return ``(kwargs, meta)``: the fftim2d.imaging kwargs and what is needed
-    to rebuild the output image, or ``-1`` on the reference's input errors."""
+    to rebuild the output image, or ``-1`` on the reference's input errors.
+    ``uvlist_device``: a CUDA device ordinal lists the uv points on that GPU
+    (``get_uvlist(device=...)``); None does it with numpy."""
     say = print if verbose else (lambda *a, **k: None)
     # Sanity checks (lbfgs.py:185-201)
     if vistable is None and amptable is None and bstable is None and catable is None:
@@ -242,7 +245,7 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
         varca = np.square(np.asarray(catable["logsigma"], dtype=np.float64))
 
     u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca = tools.get_uvlist(
-        fcvtable=vistable, amptable=amptable, bstable=bstable, catable=catable)
+        fcvtable=vistable, amptable=amptable, bstable=bstable, catable=catable, device=uvlist_device)
     u = u * (2 * np.pi * dx_rad)
     v = v * (2 * np.pi * dy_rad)
 

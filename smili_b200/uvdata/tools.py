@@ -28,46 +28,9 @@ def _cols(table, names):
     return [np.asarray(table[n]).astype(np.float64) for n in names]
 
 
-def get_uvlist(fcvtable=None, amptable=None, bstable=None, catable=None):
-    """Return ``(u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca)``.
-
-    Returns -1 (after printing an error) when no table is given, as the
-    reference does (tools.py:15-18).
-    """
-    if fcvtable is None and amptable is None and bstable is None and catable is None:
-        print("Error: No data are input.")
-        return -1
-    us, vs, ss = [], [], []
-    counts = {"fcv": 0, "amp": 0, "cp": 0, "ca": 0}
-
-    def push(u, v):
-        a, b, s = _fold(u, v)
-        us.append(a)
-        vs.append(b)
-        ss.append(s)
-
-    if fcvtable is not None:
-        u, v = _cols(fcvtable, ["u", "v"])
-        push(u, v)
-        counts["fcv"] = u.size
-    if amptable is not None:
-        u, v = _cols(amptable, ["u", "v"])
-        push(u, v)
-        counts["amp"] = u.size
-    if bstable is not None:
-        cols = _cols(bstable, ["u12", "v12", "u23", "v23", "u31", "v31"])
-        for k in range(3):
-            push(cols[2 * k], cols[2 * k + 1])
-        counts["cp"] = cols[0].size
-    if catable is not None:
-        cols = _cols(catable, ["u1", "v1", "u2", "v2", "u3", "v3", "u4", "v4"])
-        for k in range(4):
-            push(cols[2 * k], cols[2 * k + 1])
-        counts["ca"] = cols[0].size
-
-    ustack = np.concatenate(us)
-    vstack = np.concatenate(vs)
-    sstack = np.concatenate(ss)
+def _unique_host(ustack, vstack):
+    """Fold, list the distinct points (u, then v) and index them, in numpy."""
+    ustack, vstack, sstack = _fold(ustack, vstack)
     # lexicographic unique on (u, v): the order numpy uses for complex values
     order = np.lexsort((vstack, ustack))
     us_sorted, vs_sorted = ustack[order], vstack[order]
@@ -76,9 +39,67 @@ def get_uvlist(fcvtable=None, amptable=None, bstable=None, catable=None):
     rank = np.cumsum(new) - 1
     inverse = np.empty(order.size, dtype=np.int64)
     inverse[order] = rank
-    u = us_sorted[new]
-    v = vs_sorted[new]
-    uvidx = (inverse + 1) * sstack
+    return us_sorted[new], vs_sorted[new], (inverse + 1) * sstack
+
+
+def _unique_device(ustack, vstack, device):
+    """The same on the GPU (smili_get_uvlist)."""
+    import ctypes as C
+    from .. import _lib
+    u = np.ascontiguousarray(ustack, dtype=np.float64)
+    v = np.ascontiguousarray(vstack, dtype=np.float64)
+    n = u.size
+    uo, vo = np.empty(n), np.empty(n)
+    idx = np.empty(n, dtype=np.int32)
+    m = C.c_int(0)
+    opt = _lib.make_options(64, 0.0, 0, int(device))
+    _lib.check(_lib.lib().smili_get_uvlist(n, _lib.dptr(u), _lib.dptr(v), C.byref(opt), C.byref(m),
+                                           _lib.dptr(uo), _lib.dptr(vo),
+                                           idx.ctypes.data_as(C.POINTER(C.c_int))))
+    return uo[:m.value].copy(), vo[:m.value].copy(), idx.astype(np.int64)
+
+
+def get_uvlist(fcvtable=None, amptable=None, bstable=None, catable=None, device=None):
+    """Return ``(u, v, uvidxfcv, uvidxamp, uvidxcp, uvidxca)``.
+
+    ``device``: None lists the points with numpy on the host; a CUDA device
+    ordinal does the folding, sorting and indexing on that GPU
+    (``smili_get_uvlist``), with identical results.  Returns -1 (after
+    printing an error) when no table is given, as the reference does
+    (tools.py:15-18).
+    """
+    if fcvtable is None and amptable is None and bstable is None and catable is None:
+        print("Error: No data are input.")
+        return -1
+    us, vs = [], []
+    counts = {"fcv": 0, "amp": 0, "cp": 0, "ca": 0}
+    if fcvtable is not None:
+        u, v = _cols(fcvtable, ["u", "v"])
+        us.append(u)
+        vs.append(v)
+        counts["fcv"] = u.size
+    if amptable is not None:
+        u, v = _cols(amptable, ["u", "v"])
+        us.append(u)
+        vs.append(v)
+        counts["amp"] = u.size
+    if bstable is not None:
+        cols = _cols(bstable, ["u12", "v12", "u23", "v23", "u31", "v31"])
+        us.extend(cols[0::2])
+        vs.extend(cols[1::2])
+        counts["cp"] = cols[0].size
+    if catable is not None:
+        cols = _cols(catable, ["u1", "v1", "u2", "v2", "u3", "v3", "u4", "v4"])
+        us.extend(cols[0::2])
+        vs.extend(cols[1::2])
+        counts["ca"] = cols[0].size
+
+    ustack = np.concatenate(us)
+    vstack = np.concatenate(vs)
+    if device is None:
+        u, v, uvidx = _unique_host(ustack, vstack)
+    else:
+        u, v, uvidx = _unique_device(ustack, vstack, device)
 
     nf, na, nc, nq = counts["fcv"], counts["amp"], counts["cp"], counts["ca"]
     uvidxfcv = uvidx[:nf] if fcvtable is not None else np.zeros(1, dtype=np.int32)
