@@ -198,7 +198,8 @@ int smili_model_terms(const smili_imaging_args* a, const double* x, const smili_
  * folded points in u_out, v_out (capacity n) in the order np.unique gives
  * complex values (u, then v; -0 equals +0), each as first stacked; uvidx[n]
  * = sign * (1 + position of the point in that list), in stack order.
- * Device memory is allocated for the call and freed before it returns. */
+ * The library keeps a device work space per device between calls (about
+ * 100 bytes per point, grown for larger lists); calls are serialised. */
 int smili_get_uvlist(int n, const double* u, const double* v, const smili_options* opt, int* nuv,
                      double* u_out, double* v_out, int* uvidx);
 

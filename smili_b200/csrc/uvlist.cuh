@@ -14,6 +14,7 @@
 // where the key changes, a three-kernel scan of the flags into list
 // positions, and two scatters.  Included by solver.cu (error reporting).
 #pragma once
+#include <mutex>
 
 struct UvKey {
   unsigned long long ku, kv;
@@ -197,8 +198,18 @@ __global__ void uv_sign(int n, const int* inv, const signed char* sg, int* uvidx
     uvidx[i] = (int)sg[i] * (inv[i] + 1);
 }
 
+// Device work space per device, kept between calls and grown when a larger
+// list arrives (allocation and release of tens of MB cost up to tens of ms
+// each, more than the listing itself).  Calls hold g_uv_mu for their whole
+// duration, so the space is never shared by two calls at once.
+struct UvWork {
+  char* d = nullptr;
+  size_t cap = 0;
+};
+static std::mutex g_uv_mu;
+static UvWork g_uv_work[64];
+
 // Host side: validates, runs the kernels on `st` and copies the results back.
-// Device buffers are allocated per call and freed before returning.
 static int uvlist_run(int n, const double* u, const double* v, int device, cudaStream_t st, int* nuv,
                       double* u_out, double* v_out, int* uvidx) {
   if (n < 1 || n > (1 << 26) || !u || !v || !nuv || !u_out || !v_out || !uvidx)
@@ -207,8 +218,9 @@ static int uvlist_run(int n, const double* u, const double* v, int device, cudaS
     if (!std::isfinite(u[i]) || !std::isfinite(v[i])) return fail(SMILI_ERR_DATA, "get_uvlist: non-finite u or v");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SMILI_ERR_NODEV, "no CUDA device");
-  if (device < 0 || device >= ndev || cudaSetDevice(device) != cudaSuccess)
+  if (device < 0 || device >= ndev || device >= 64 || cudaSetDevice(device) != cudaSuccess)
     return fail(SMILI_ERR_NODEV, "cannot select the CUDA device");
+  std::lock_guard<std::mutex> lock(g_uv_mu);
   long npad = UV_BLK;
   while (npad < n) npad <<= 1;
   const int nb = (n + UV_SCAN - 1) / UV_SCAN;
@@ -224,8 +236,19 @@ static int uvlist_run(int n, const double* u, const double* v, int device, cudaS
                o_bsum = take(4 * (size_t)nb), o_inv = take(4 * (size_t)n), o_uo = take(8 * (size_t)n),
                o_vo = take(8 * (size_t)n), o_idx = take(4 * (size_t)n), o_u = take(8 * (size_t)n),
                o_v = take(8 * (size_t)n);
-  char* d = nullptr;
-  if (cudaMalloc(&d, off) != cudaSuccess) return fail(SMILI_ERR_CUDA, "get_uvlist: cudaMalloc failed");
+  UvWork& wk = g_uv_work[device];
+  if (wk.cap < off) {
+    if (wk.d) cudaFree(wk.d);
+    wk.d = nullptr;
+    wk.cap = 0;
+    const size_t want = off + off / 4;  // headroom for slightly larger lists
+    if (cudaMalloc(&wk.d, want) != cudaSuccess) {
+      wk.d = nullptr;
+      return fail(SMILI_ERR_CUDA, "get_uvlist: cudaMalloc of the work space failed");
+    }
+    wk.cap = want;
+  }
+  char* d = wk.d;
   auto at_ = [&](size_t o) { return d + o; };
   UvKey* keys = reinterpret_cast<UvKey*>(at_(o_keys));
   double *fu = reinterpret_cast<double*>(at_(o_fu)), *fv = reinterpret_cast<double*>(at_(o_fv));
@@ -277,7 +300,6 @@ static int uvlist_run(int n, const double* u, const double* v, int device, cudaS
     chk(cudaMemcpyAsync(uvidx, idx, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
     chk(cudaStreamSynchronize(st));
   }
-  cudaFree(d);
   if (e != cudaSuccess) return fail(SMILI_ERR_CUDA, std::string("get_uvlist: ") + cudaGetErrorString(e));
   *nuv = m;
   return SMILI_OK;
