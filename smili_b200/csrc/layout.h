@@ -83,6 +83,15 @@ struct ProbDesc {
   int64_t o_out;                        // results: terms[15], counters
 };
 
+// every arena offset of ProbDesc, for code that moves a problem's region
+#define SMILI_PROB_OFFSETS(X)                                                                          \
+  X(o_x0) X(o_xidx) X(o_yidx) X(o_inv) X(o_xg) X(o_ex) X(o_ey) X(o_l1w) X(o_tvw) X(o_tsvw) X(o_klw)  \
+  X(o_gsw) X(o_dc1) X(o_dc2) X(o_tw1) X(o_tw2) X(o_u) X(o_v) X(o_dre) X(o_dim) X(o_dvar) X(o_didx)   \
+  X(o_dsgn) X(o_csr_off) X(o_csr_ent) X(o_items) X(o_tmpA) X(o_bandA) X(o_V) X(o_contrib) X(o_bandC) \
+  X(o_tmpC) X(o_gchi) X(o_part) X(o_x) X(o_g) X(o_z) X(o_r) X(o_d) X(o_t) X(o_xp) X(o_ws) X(o_wy)     \
+  X(o_iwh) X(o_free) X(o_bkey) X(o_sbk) X(o_sbi) X(o_hist) X(o_cand) X(o_lred) X(o_state) X(o_trace) \
+  X(o_model) X(o_frames) X(o_rtw) X(o_riw) X(o_lcf) X(o_iavg) X(o_out)
+
 // Scalar L-BFGS-B state (setulb's isave/dsave/lsave plus the small matrices).
 struct LbState {
   int task, done, error;

@@ -8,12 +8,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/smili_b200.h"
@@ -1067,21 +1069,49 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   b->prec64 = sizeof(R) == 8;
   b->device = device;
   b->kind = kind;
-  Arena ar;
+  // The problems are packed in parallel on the host cores, each into its own
+  // arena region (starting with a 256-byte reserve, so no present field sits
+  // at offset 0, the mark of an absent one); the regions are then laid end
+  // to end and every offset moved by its region's start.
+  std::vector<Arena> ars(nprob);
   std::vector<HostProb> hps(nprob);
-  int maxn = 1;
-  for (int p = 0; p < nprob; ++p) {
-    const int rc = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ar,
-                                   hps[p], x_over ? x_over[p] : nullptr, c_re, c_im, 0.0,
-                                   opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
-    if (rc != SMILI_OK) {
-      delete b;
-      return rc;
+  std::vector<int> rcs(nprob, SMILI_OK);
+  std::vector<std::string> errs(nprob);
+  std::atomic<int> next{0};
+  auto work = [&]() {
+    for (int p = next.fetch_add(1); p < nprob; p = next.fetch_add(1)) {
+      ars[p].take(256);
+      rcs[p] = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ars[p],
+                               hps[p], x_over ? x_over[p] : nullptr, c_re, c_im, 0.0,
+                               opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
+      if (rcs[p] != SMILI_OK) errs[p] = g_err;
     }
-    b->descs.push_back(hps[p].d);
-    maxn = std::max(maxn, hps[p].d.npix);
+  };
+  const int nth = std::max(1, std::min(nprob, (int)std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nth; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  for (int p = 0; p < nprob; ++p)
+    if (rcs[p] != SMILI_OK) {
+      delete b;
+      return fail(rcs[p], errs[p]);
+    }
+  int maxn = 1;
+  size_t base = 0;
+  for (int p = 0; p < nprob; ++p) {
+    ProbDesc& d = hps[p].d;
+#define SMILI_MOVE(f) \
+  if (d.f) d.f += (int64_t)base;
+    SMILI_PROB_OFFSETS(SMILI_MOVE)
+#undef SMILI_MOVE
+    for (auto& bl : hps[p].blobs)
+      if (bl.first >= 0) bl.first += (int64_t)base;
+    base += ars[p].bytes;
+    b->descs.push_back(d);
+    maxn = std::max(maxn, d.npix);
   }
-  b->arena_bytes = ar.bytes;
+  b->arena_bytes = base;
   return finish_batch<R>(b, hps, maxn, opt, out);
 }
 
