@@ -71,3 +71,19 @@ def test_movie_closure_across_frames_rejected():
     with pytest.raises(_lib.SmiliError) as e:
         fftim3d.calc_cost(kw["iin"], **bad)
     assert e.value.code == -6
+
+
+def test_batch_packing_reports_the_failing_problem_without_device(crescent32, closure40):
+    """Problems of a batch are packed in parallel on the host; a bad problem
+    in the middle of the batch fails the whole creation with its own error
+    code and message, before any device is touched."""
+    from smili_b200 import _lib
+    good = make_kw(crescent32)
+    bad = dict(make_kw(closure40))
+    bad["varamp"] = np.asarray(bad["varamp"]).copy()
+    bad["varamp"][3] = -1.0  # a non-positive variance
+    probs = [_lib.Problem(good), _lib.Problem(good), _lib.Problem(bad), _lib.Problem(good)]
+    with pytest.raises(_lib.SmiliError) as e:
+        _lib.Batch(probs, niter=5, options=_lib.make_options(64, 1e-6))
+    assert e.value.code == -2
+    assert "varia" in str(e.value).lower()
