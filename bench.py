@@ -221,6 +221,45 @@ def warm_start_cfg4(nprob, niter, rtol, device=0, group=4):
             "nrmse_truth_warm_fp32": nr(xs_w)}
 
 
+def survey_cfg3(nprob, niter, device=0, nplain=8):
+    """The batched survey: nprob problems with image sizes from {64, 96, 128,
+    192, 256}^2, 2e3-5e4 visibilities, fcv + closure phases and (l1, tsv, mem)
+    on the 8^3 log grid, solved in one launch in FP32 and in FP64 (the faster
+    of two launches each), and the plain method (one FP64 launch per problem)
+    on the first nplain problems."""
+    from smili_b200 import _lib, synth
+    from smili_b200.imaging.lbfgs import prepare_imaging
+    kws = []
+    for i in range(nprob):
+        obs = synth.survey_problem(i, seed=3, niter=niter, model=synth.nufft_model)
+        kw, _ = prepare_imaging(obs.image, vistable=obs.vistable, bstable=obs.bstable, niter=niter, **obs.reg)
+        kws.append(kw)
+    probs = [_lib.Problem(k) for k in kws]
+    out = {"problems": nprob, "niter": niter,
+           "nx_counts": {str(n): int(sum(int(k["nx"]) == n for k in kws)) for n in (64, 96, 128, 192, 256)},
+           "uv_points_median": int(np.median([np.size(k["u"]) for k in kws]))}
+    cost = {}
+    for prec in (32, 64):
+        b = _lib.Batch(probs, niter=niter, options=_lib.make_options(prec, 1e-6, 0, device))
+        ms = min(b.run(), b.run())
+        info = [b.fetch(p)[3] for p in range(nprob)]
+        cost[prec] = np.array([b.fetch(p)[1]["cost"] for p in range(nprob)])
+        b.close()
+        out[f"fp{prec}_batched_s"] = ms / 1e3
+        out[f"fp{prec}_batched_solves_per_s"] = nprob / (ms / 1e3)
+        out[f"fp{prec}_iterations_mean"] = float(np.mean([i["niter"] for i in info]))
+    r = cost[32] / cost[64]
+    out["fp32_over_fp64_final_cost_median_p10_p90"] = [float(np.median(r)), float(np.percentile(r, 10)),
+                                                       float(np.percentile(r, 90))]
+    ts = []
+    for p in range(min(nplain, nprob)):
+        s = _lib.Batch([probs[p]], niter=niter, options=_lib.make_options(64, 1e-6, 0, device))
+        ts.append(s.run())
+        s.close()
+    out["plain_fp64_single_solves_per_s"] = 1e3 / float(np.mean(ts))
+    return out
+
+
 def dynamic_cfg5(niter, device=0, cpu_evals=2):
     """Dynamic imaging (fftim3d): 64 frames of 128x128, ~6000 visibilities
     per frame from 16 stations over 24 h, a crescent rotating by 90 deg,
@@ -358,6 +397,8 @@ def main():
     ap.add_argument("--ctas", type=int, default=None,
                     help="fixed CTAs per problem instead of the autotuner (profiled runs: the autotuner's "
                          "timings are not meaningful under a profiler)")
+    ap.add_argument("--survey", type=int, default=0,
+                    help="also measure the batched survey with this many problems (512: the survey configuration)")
     ap.add_argument("--config5", action="store_true",
                     help="also solve the 64-frame movie and the 1024x1024 / 2e6-visibility image")
     ap.add_argument("--warm-problems", type=int, default=256,
@@ -545,6 +586,8 @@ def main():
         if args.config5:
             line["dynamic_cfg5"] = dynamic_cfg5(args.niter, local)
             line["large_cfg5"] = large_cfg5(args.niter, local)
+        if args.survey > 0:
+            line["survey_cfg3"] = survey_cfg3(args.survey, args.niter, local)
         if args.warm_problems > 0:
             line["warm_start_cfg4"] = warm_start_cfg4(args.warm_problems, args.niter, args.target_rtol, local)
         if not args.no_cpu:
