@@ -112,7 +112,9 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
         yidx = yidx.reshape(Nyx)
         winidx = None
     else:
-        if hasattr(imregion, "imagewin"):
+        if isinstance(imregion, np.ndarray):  # a (ny, nx) mask (ndarray also has .data)
+            imagewin = imregion.astype(bool)
+        elif hasattr(imregion, "imagewin"):
             imagewin = imregion.imagewin(initimage, istokes, ifreq)
         elif hasattr(imregion, "data"):
             imagewin = imregion.data[0, 0] > 0.5

@@ -66,7 +66,9 @@ def prepare_imaging3d(initmovie, imregion=None, vistable=None, amptable=None, bs
         xidx, yidx = xidx.reshape(Nyx), yidx.reshape(Nyx)
         winidx = None
     else:
-        if hasattr(imregion, "imagewin"):
+        if isinstance(imregion, np.ndarray):  # a (ny, nx) mask (ndarray also has .data)
+            imagewin = imregion.astype(bool)
+        elif hasattr(imregion, "imagewin"):
             imagewin = imregion.imagewin(init0, istokes, ifreq)
         elif hasattr(imregion, "data"):
             imagewin = imregion.data[0, 0] > 0.5

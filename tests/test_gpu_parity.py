@@ -178,6 +178,38 @@ def test_solve_per_iteration_matches_oracle(oracle, crescent32, lib):
     assert abs(terms["cost"] - tref["cost"]) <= 1e-4 * abs(tref["cost"])
 
 
+def _window(n, r):
+    yy, xx = np.mgrid[:n, :n]
+    return (xx - n // 2) ** 2 + (yy - n // 2) ** 2 < r * r
+
+
+@pytest.mark.parametrize("variant", ["m1", "m3", "m6", "unbounded", "window"])
+def test_solve_variants_match_oracle(oracle, crescent32, lib, variant):
+    """The optimiser's other settings against the oracle, per iteration (FP64):
+    L-BFGS-B memories 1, 3 and 6 (the largest the device accepts), no
+    non-negativity bound (the unconstrained path: no Cauchy search), and a
+    windowed pixel set (a disc of 13 pixels radius in the 32 x 32 grid)."""
+    over = {"niter": 20}
+    if variant == "window":
+        over["imregion"] = _window(32, 13)
+    kw = make_kw(crescent32, **over)
+    if variant.startswith("m"):
+        kw["m"] = int(variant[1:])
+    if variant == "unbounded":
+        kw["nonneg"] = False
+    if variant == "window":
+        assert kw["npix"] == int(_window(32, 13).sum()) < 32 * 32
+    b = lib.Batch([kw], niter=20, nonneg=kw["nonneg"], m=kw["m"], options=lib.make_options(64, 1e-12))
+    b.run()
+    _, terms, _, info = b.fetch(0)
+    tr = b.trace(0, 22)
+    b.close()
+    _, tref, iref = oracle.imaging(kw, eps=1e-12)
+    assert info["niter"] == iref["niter"]
+    np.testing.assert_allclose(tr[:10], iref["trace"][:10], rtol=1e-9)
+    np.testing.assert_allclose(tr[:20], iref["trace"][:20], rtol=2e-5)
+
+
 def test_solve_closure_terms_matches_oracle(oracle, closure40, lib):
     kw = make_kw(closure40, niter=40)
     b = lib.Batch([kw], niter=40, options=lib.make_options(64, 1e-12))
