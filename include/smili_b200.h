@@ -108,7 +108,11 @@ int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const 
                        smili_batch** out);
 /* Solve (fg_only = 0) or evaluate calc_cost once (fg_only = 1) for every
  * problem on the device; fg_only = 2 only times 1000 group barriers (a
- * diagnostic).  kernel_ms (optional) receives the device time of the launch. */
+ * diagnostic); fg_only = 3 checks the bounded waits: one CTA of every group
+ * skips a group barrier, the others give up after about 10 ms and the call
+ * returns SMILI_ERR_TIMEOUT (with one CTA per problem there is no group
+ * barrier to miss and it returns SMILI_OK).  The batch stays usable.
+ * kernel_ms (optional) receives the device time of the launch. */
 int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms);
 int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double* grad,
                       smili_solve_info* info);

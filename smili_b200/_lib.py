@@ -271,9 +271,10 @@ class Batch:
 
     def run(self, fg_only=False):
         """Run on the device; returns the launch's device time in ms.
-        fg_only: False solve, True one evaluation, 2 time 1000 group barriers."""
+        fg_only: False solve, True one evaluation, 2 time 1000 group barriers,
+        3 check the bounded waits (a barrier one CTA skips: SMILI_ERR_TIMEOUT)."""
         ms = C.c_float(0.0)
-        mode = 2 if fg_only == 2 else int(bool(fg_only))
+        mode = fg_only if fg_only in (2, 3) else int(bool(fg_only))
         check(lib().smili_batch_run(self.h, mode, C.byref(ms)))
         return float(ms.value)
 

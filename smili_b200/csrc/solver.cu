@@ -29,7 +29,11 @@
 #define SMILI_SMEM_CPX 2048   // complex elements per FFT buffer
 #define SMILI_DYN_CPX 6144    // complex elements of dynamic shared memory (96 KB FP64)
 
-enum { MODE_SOLVE = 0, MODE_FG = 1, MODE_T2 = 2, MODE_T1 = 3, MODE_BARRIER = 4 };
+enum { MODE_SOLVE = 0, MODE_FG = 1, MODE_T2 = 2, MODE_T1 = 3, MODE_BARRIER = 4, MODE_WAIT_LIMIT = 5 };
+
+// polls of a group-barrier wait in the wait-limit check (MODE_WAIT_LIMIT):
+// about 10 ms, instead of the seconds a real barrier may wait
+#define SMILI_TEST_SPIN_LIMIT (1LL << 14)
 
 struct BatchArgs {
   char* arena;
@@ -315,6 +319,14 @@ __global__ void __launch_bounds__(Shape<R>::threads, Shape<R>::min_blocks) smili
   if (a.mode == MODE_BARRIER) {  // cost of the group barrier: 1000 waits
     for (int i = 0; i < 1000; ++i)
       if (!group_sync(g)) return;
+    return;
+  }
+  if (a.mode == MODE_WAIT_LIMIT) {
+    // check of the bounded waits: rank 0 of every group never arrives at the
+    // barrier, so the others' waits run out after a short limit, set the
+    // abort flag and return; the host then reports SMILI_ERR_TIMEOUT
+    g.spin_limit = SMILI_TEST_SPIN_LIMIT;
+    if (rank != 0) group_sync(g);
     return;
   }
   while (true) {
@@ -1568,6 +1580,7 @@ int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const 
 int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms) {
   if (!b) return fail(SMILI_ERR_ARG, "null batch");
   if (fg_only == 2) return run(b, MODE_BARRIER, kernel_ms);  // barrier timing (diagnostic)
+  if (fg_only == 3) return run(b, MODE_WAIT_LIMIT, kernel_ms);  // bounded-wait check (diagnostic)
   return run(b, fg_only ? MODE_FG : MODE_SOLVE, kernel_ms);
 }
 
