@@ -35,3 +35,27 @@ def test_one_cta_per_problem_has_no_barrier_to_miss(crescent32):
     b = _lib.Batch([kw], niter=5, options=_lib.make_options(64, 1e-9, 1))
     b.run(3)  # G == 1: block barriers only, nothing to time out
     b.close()
+
+
+def test_non_finite_problem_is_contained(oracle, closure40):
+    """A problem whose objective is not finite (closure amplitudes of an
+    all-zero start image: log |V| = -inf) ends as the oracle's does, and the
+    problems beside it in the batch are unaffected."""
+    from smili_b200 import _lib
+    kw = make_kw(closure40, niter=20)
+    bad = dict(kw, iin=np.zeros_like(kw["iin"]))
+    _, tref, iref = oracle.imaging(bad, eps=1e-12)
+    assert not np.isfinite(tref["cost"])
+    single = _lib.Batch([kw], niter=20, options=_lib.make_options(64, 1e-12))
+    single.run()
+    good_cost = single.fetch(0)[1]["cost"]
+    single.close()
+    b = _lib.Batch([kw, bad, kw], niter=20, options=_lib.make_options(64, 1e-12))
+    b.run()
+    _, tb, _, ib = b.fetch(1)
+    assert not np.isfinite(tb["cost"])
+    assert ib["task"] == iref["task"] and ib["niter"] == iref["niter"]
+    for p in (0, 2):
+        _, t, _, _ = b.fetch(p)
+        assert abs(t["cost"] - good_cost) <= 1e-6 * abs(good_cost)
+    b.close()
