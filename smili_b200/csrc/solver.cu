@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -1092,11 +1093,16 @@ int create_batch(int nprob, const smili_imaging_args* const* probs, const int* n
   std::atomic<int> next{0};
   auto work = [&]() {
     for (int p = next.fetch_add(1); p < nprob; p = next.fetch_add(1)) {
-      ars[p].take(256);
-      rcs[p] = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ars[p],
-                               hps[p], x_over ? x_over[p] : nullptr, c_re, c_im, 0.0,
-                               opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
-      if (rcs[p] != SMILI_OK) errs[p] = g_err;
+      try {  // an exception must not leave a worker thread (std::terminate)
+        ars[p].take(256);
+        rcs[p] = pack_problem<R>(*probs[p], kind, niter ? niter[p] : 0, nonneg, m, factr, pgtol, eps, ars[p],
+                                 hps[p], x_over ? x_over[p] : nullptr, c_re, c_im, 0.0,
+                                 opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
+        if (rcs[p] != SMILI_OK) errs[p] = g_err;
+      } catch (const std::exception& ex) {
+        rcs[p] = SMILI_ERR_ARG;
+        errs[p] = std::string("host packing of a problem failed: ") + ex.what();
+      }
     }
   };
   const int nth = std::max(1, std::min(nprob, (int)std::thread::hardware_concurrency()));
