@@ -26,6 +26,7 @@ extern "C" {
 #define SMILI_ERR_NODEV (-4)       /* no usable CUDA device */
 #define SMILI_ERR_TIMEOUT (-5)     /* a device-side wait gave up (solve aborted) */
 #define SMILI_ERR_UNSUPPORTED (-6) /* e.g. L-BFGS-B memory m > 6 */
+#define SMILI_ERR_HOST (-7)        /* host-side failure, e.g. out of host memory */
 
 /* Solver task codes reported in smili_solve_info.task */
 #define SMILI_TASK_CONV 3      /* CONVERGENCE: pgtol or factr test */

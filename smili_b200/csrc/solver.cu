@@ -1569,6 +1569,22 @@ int create_any(int nprob, const smili_imaging_args* const* probs, const int* nit
 
 }  // namespace
 
+// Every C-ABI entry point runs its body through guarded(): a C++ exception
+// (host allocation failure, mostly) becomes SMILI_ERR_HOST with a message
+// instead of unwinding into the C caller.
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    return fail(SMILI_ERR_HOST, "out of host memory");
+  } catch (const std::exception& e) {
+    return fail(SMILI_ERR_HOST, std::string("host failure: ") + e.what());
+  } catch (...) {
+    return fail(SMILI_ERR_HOST, "host failure");
+  }
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -1579,67 +1595,79 @@ int smili_version(void) { return SMILI_VERSION; }
 
 int smili_batch_create(int nprob, const smili_imaging_args* const* probs, const int* niter, int nonneg,
                        int m, double factr, double pgtol, const smili_options* opt, smili_batch** out) {
-  return create_any(nprob, probs, niter, nonneg, m, factr, pgtol, opt, PK_SOLVE, nullptr, nullptr, nullptr,
-                    out);
+  return guarded([&]() -> int {
+    return create_any(nprob, probs, niter, nonneg, m, factr, pgtol, opt, PK_SOLVE, nullptr, nullptr, nullptr,
+                      out);
+  });
 }
 
 int smili_batch_run(smili_batch* b, int fg_only, float* kernel_ms) {
-  if (!b) return fail(SMILI_ERR_ARG, "null batch");
-  if (fg_only == 2) return run(b, MODE_BARRIER, kernel_ms);  // barrier timing (diagnostic)
-  if (fg_only == 3) return run(b, MODE_WAIT_LIMIT, kernel_ms);  // bounded-wait check (diagnostic)
-  return run(b, fg_only ? MODE_FG : MODE_SOLVE, kernel_ms);
+  return guarded([&]() -> int {
+    if (!b) return fail(SMILI_ERR_ARG, "null batch");
+    if (fg_only == 2) return run(b, MODE_BARRIER, kernel_ms);  // barrier timing (diagnostic)
+    if (fg_only == 3) return run(b, MODE_WAIT_LIMIT, kernel_ms);  // bounded-wait check (diagnostic)
+    return run(b, fg_only ? MODE_FG : MODE_SOLVE, kernel_ms);
+  });
 }
 
 int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double* grad,
                       smili_solve_info* info) {
-  if (!b || p < 0 || p >= b->nprob) return fail(SMILI_ERR_ARG, "invalid problem index");
-  CUDA_TRY(cudaSetDevice(b->device));
-  const ProbDesc& d = b->descs[p];
-  if (iout) CUDA_TRY(cudaMemcpy(iout, b->d_arena + d.o_x, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
-  if (grad) CUDA_TRY(cudaMemcpy(grad, b->d_arena + d.o_g, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
-  ProbResult r;
-  CUDA_TRY(cudaMemcpy(&r, b->d_results + p, sizeof(r), cudaMemcpyDeviceToHost));
-  if (terms) std::memcpy(terms, r.terms, sizeof(double) * (d.nframes > 0 ? SMILI_NTERMS3D : SMILI_NTERMS));
-  if (info) {
-    info->task = r.task;
-    info->niter = r.iter;
-    info->nfg = r.nfg;
-    info->error = r.error;
-  }
-  return SMILI_OK;
+  return guarded([&]() -> int {
+    if (!b || p < 0 || p >= b->nprob) return fail(SMILI_ERR_ARG, "invalid problem index");
+    CUDA_TRY(cudaSetDevice(b->device));
+    const ProbDesc& d = b->descs[p];
+    if (iout) CUDA_TRY(cudaMemcpy(iout, b->d_arena + d.o_x, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
+    if (grad) CUDA_TRY(cudaMemcpy(grad, b->d_arena + d.o_g, sizeof(double) * d.npix, cudaMemcpyDeviceToHost));
+    ProbResult r;
+    CUDA_TRY(cudaMemcpy(&r, b->d_results + p, sizeof(r), cudaMemcpyDeviceToHost));
+    if (terms) std::memcpy(terms, r.terms, sizeof(double) * (d.nframes > 0 ? SMILI_NTERMS3D : SMILI_NTERMS));
+    if (info) {
+      info->task = r.task;
+      info->niter = r.iter;
+      info->nfg = r.nfg;
+      info->error = r.error;
+    }
+    return SMILI_OK;
+  });
 }
 
 int smili_batch_profile(smili_batch* b, int enable, double* stage_ns, int len) {
-  if (!b) return fail(SMILI_ERR_ARG, "null batch");
-  b->profile = enable ? 1 : 0;
-  if (stage_ns && len > 0) {
-    unsigned long long h[PR_NSTAGE];
-    CUDA_TRY(cudaSetDevice(b->device));
-    CUDA_TRY(cudaMemcpy(h, b->d_prof, sizeof(h), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < len; ++i) stage_ns[i] = i < PR_NSTAGE ? (double)h[i] : 0.0;
-  }
-  return SMILI_OK;
+  return guarded([&]() -> int {
+    if (!b) return fail(SMILI_ERR_ARG, "null batch");
+    b->profile = enable ? 1 : 0;
+    if (stage_ns && len > 0) {
+      unsigned long long h[PR_NSTAGE];
+      CUDA_TRY(cudaSetDevice(b->device));
+      CUDA_TRY(cudaMemcpy(h, b->d_prof, sizeof(h), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < len; ++i) stage_ns[i] = i < PR_NSTAGE ? (double)h[i] : 0.0;
+    }
+    return SMILI_OK;
+  });
 }
 
 int smili_batch_set_targets(smili_batch* b, const double* ftarget) {
-  if (!b) return fail(SMILI_ERR_ARG, "null batch");
-  for (int p = 0; p < b->nprob; ++p) b->descs[p].ftarget = ftarget ? ftarget[p] : -INFINITY;
-  CUDA_TRY(cudaSetDevice(b->device));
-  CUDA_TRY(cudaMemcpyAsync(b->d_descs, b->descs.data(), sizeof(ProbDesc) * b->nprob, cudaMemcpyHostToDevice,
-                           b->stream));
-  CUDA_TRY(cudaStreamSynchronize(b->stream));
-  return SMILI_OK;
+  return guarded([&]() -> int {
+    if (!b) return fail(SMILI_ERR_ARG, "null batch");
+    for (int p = 0; p < b->nprob; ++p) b->descs[p].ftarget = ftarget ? ftarget[p] : -INFINITY;
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaMemcpyAsync(b->d_descs, b->descs.data(), sizeof(ProbDesc) * b->nprob, cudaMemcpyHostToDevice,
+                             b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return SMILI_OK;
+  });
 }
 
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len) {
-  if (!b || p < 0 || p >= b->nprob || !trace) return fail(SMILI_ERR_ARG, "invalid trace request");
-  const ProbDesc& d = b->descs[p];
-  if (!d.o_trace) return fail(SMILI_ERR_ARG, "no trace for this batch");
-  const int n = std::min(len, d.niter + 2);
-  CUDA_TRY(cudaSetDevice(b->device));
-  CUDA_TRY(cudaMemcpy(trace, b->d_arena + d.o_trace, sizeof(double) * n, cudaMemcpyDeviceToHost));
-  for (int i = n; i < len; ++i) trace[i] = NAN;
-  return SMILI_OK;
+  return guarded([&]() -> int {
+    if (!b || p < 0 || p >= b->nprob || !trace) return fail(SMILI_ERR_ARG, "invalid trace request");
+    const ProbDesc& d = b->descs[p];
+    if (!d.o_trace) return fail(SMILI_ERR_ARG, "no trace for this batch");
+    const int n = std::min(len, d.niter + 2);
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaMemcpy(trace, b->d_arena + d.o_trace, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    for (int i = n; i < len; ++i) trace[i] = NAN;
+    return SMILI_OK;
+  });
 }
 
 void smili_batch_destroy(smili_batch* b) {
@@ -1655,105 +1683,115 @@ void smili_batch_destroy(smili_batch* b) {
 int smili_fftim2d_imaging(const smili_imaging_args* a, int niter, int nonneg, int nprint, int m, double factr,
                           double pgtol, const smili_options* opt, double* iout, double* terms,
                           smili_solve_info* info) {
-  (void)nprint;  // progress prints re-evaluate the cost at the same image; no effect on the result
-  if (!a || !iout) return fail(SMILI_ERR_ARG, "null argument");
-  if (niter < 0) return fail(SMILI_ERR_ARG, "niter must be >= 0");
-  smili_batch* b = nullptr;
-  const smili_imaging_args* probs[1] = {a};
-  int rc = create_any(1, probs, &niter, nonneg, m, factr, pgtol, opt, PK_SOLVE, nullptr, nullptr, nullptr, &b);
-  if (rc != SMILI_OK) return rc;
-  rc = run(b, MODE_SOLVE, nullptr);
-  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, iout, terms, nullptr, info);
-  smili_batch_destroy(b);
-  return rc;
+  return guarded([&]() -> int {
+    (void)nprint;  // progress prints re-evaluate the cost at the same image; no effect on the result
+    if (!a || !iout) return fail(SMILI_ERR_ARG, "null argument");
+    if (niter < 0) return fail(SMILI_ERR_ARG, "niter must be >= 0");
+    smili_batch* b = nullptr;
+    const smili_imaging_args* probs[1] = {a};
+    int rc = create_any(1, probs, &niter, nonneg, m, factr, pgtol, opt, PK_SOLVE, nullptr, nullptr, nullptr, &b);
+    if (rc != SMILI_OK) return rc;
+    rc = run(b, MODE_SOLVE, nullptr);
+    if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, iout, terms, nullptr, info);
+    smili_batch_destroy(b);
+    return rc;
+  });
 }
 
 int smili_calc_cost(const smili_imaging_args* a, const double* x, const smili_options* opt, double* terms,
                     double* grad) {
-  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
-  smili_batch* b = nullptr;
-  const smili_imaging_args* probs[1] = {a};
-  const double* xo[1] = {x};
-  int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_FG, xo, nullptr, nullptr, &b);
-  if (rc != SMILI_OK) return rc;
-  rc = run(b, MODE_FG, nullptr);
-  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
-  smili_batch_destroy(b);
-  return rc;
+  return guarded([&]() -> int {
+    if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+    smili_batch* b = nullptr;
+    const smili_imaging_args* probs[1] = {a};
+    const double* xo[1] = {x};
+    int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_FG, xo, nullptr, nullptr, &b);
+    if (rc != SMILI_OK) return rc;
+    rc = run(b, MODE_FG, nullptr);
+    if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
+    smili_batch_destroy(b);
+    return rc;
+  });
 }
 
 int smili_fftim3d_imaging(const smili_imaging3d_args* a, int niter, int nonneg, int nprint, int m, double factr,
                           double pgtol, const smili_options* opt, double* iout, double* terms3d,
                           smili_solve_info* info) {
-  (void)nprint;  // progress prints re-evaluate the cost at the same movie; no effect on the result
-  if (!a || !iout) return fail(SMILI_ERR_ARG, "null argument");
-  if (niter < 0) return fail(SMILI_ERR_ARG, "niter must be >= 0");
-  smili_batch* b = nullptr;
-  int rc = create_movie_any(a, PK_SOLVE, niter, nonneg, m, factr, pgtol, opt, nullptr, &b);
-  if (rc != SMILI_OK) return rc;
-  rc = run(b, MODE_SOLVE, nullptr);
-  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, iout, terms3d, nullptr, info);
-  smili_batch_destroy(b);
-  if (rc == SMILI_OK) {
-    const size_t n = (size_t)a->npix * a->nz;
-    for (size_t i = 0; i < n; ++i)
-      if (std::fabs(iout[i]) < 1e-10) iout[i] = 0.0;  // fftim3d.f90:466 (zeroeps)
-  }
-  return rc;
+  return guarded([&]() -> int {
+    (void)nprint;  // progress prints re-evaluate the cost at the same movie; no effect on the result
+    if (!a || !iout) return fail(SMILI_ERR_ARG, "null argument");
+    if (niter < 0) return fail(SMILI_ERR_ARG, "niter must be >= 0");
+    smili_batch* b = nullptr;
+    int rc = create_movie_any(a, PK_SOLVE, niter, nonneg, m, factr, pgtol, opt, nullptr, &b);
+    if (rc != SMILI_OK) return rc;
+    rc = run(b, MODE_SOLVE, nullptr);
+    if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, iout, terms3d, nullptr, info);
+    smili_batch_destroy(b);
+    if (rc == SMILI_OK) {
+      const size_t n = (size_t)a->npix * a->nz;
+      for (size_t i = 0; i < n; ++i)
+        if (std::fabs(iout[i]) < 1e-10) iout[i] = 0.0;  // fftim3d.f90:466 (zeroeps)
+    }
+    return rc;
+  });
 }
 
 int smili_calc_cost3d(const smili_imaging3d_args* a, const double* x, const smili_options* opt, double* terms3d,
                       double* grad) {
-  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
-  smili_batch* b = nullptr;
-  int rc = create_movie_any(a, PK_FG, 0, 0, 5, 1e1, 0.0, opt, x, &b);
-  if (rc != SMILI_OK) return rc;
-  rc = run(b, MODE_FG, nullptr);
-  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms3d, grad, nullptr);
-  smili_batch_destroy(b);
-  return rc;
+  return guarded([&]() -> int {
+    if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+    smili_batch* b = nullptr;
+    int rc = create_movie_any(a, PK_FG, 0, 0, 5, 1e1, 0.0, opt, x, &b);
+    if (rc != SMILI_OK) return rc;
+    rc = run(b, MODE_FG, nullptr);
+    if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms3d, grad, nullptr);
+    smili_batch_destroy(b);
+    return rc;
+  });
 }
 
 int smili_model_terms(const smili_imaging_args* a, const double* x, const smili_options* opt, double* chisq,
                       double* grad, double* model_re, double* model_im, double* resid_re, double* resid_im) {
-  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
-  const int prec = opt && opt->precision ? opt->precision : 64;
-  if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
-  smili_batch* b = nullptr;
-  int rc = prec == 64 ? create_model<double>(*a, x, opt, &b) : create_model<float>(*a, x, opt, &b);
-  if (rc != SMILI_OK) return rc;
-  rc = run(b, MODE_FG, nullptr);
-  double terms[SMILI_NTERMS];
-  if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
-  if (rc == SMILI_OK) {
-    const ProbDesc& d = b->descs[0];
-    std::vector<double> mr(4 * (size_t)d.ndata);
-    cudaError_t e = cudaMemcpy(mr.data(), b->d_arena + d.o_model, sizeof(double) * mr.size(), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) {
-      rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
-    } else {
-      if (chisq) *chisq = terms[0];
-      const double dix = a->nx / 2.0 + 1 - a->nxref, diy = a->ny / 2.0 + 1 - a->nyref;
-      for (int i = 0; i < d.ndata; ++i) {
-        std::complex<double> mo(mr[4 * i], mr[4 * i + 1]), re(mr[4 * i + 2], mr[4 * i + 3]);
-        if (a->isfcv) {  // phashift_c2r (fftlib.f90:200-220) of model and residual
-          const int k = std::abs(a->uvidxfcv[i]) - 1, sg = a->uvidxfcv[i] > 0 ? 1 : -1;
-          const std::complex<double> ph = std::exp(std::complex<double>(0.0, a->u[k] * sg * dix + a->v[k] * sg * diy));
-          mo *= ph;
-          re *= ph;
-        } else if (a->iscp) {  // model_cp wraps both into (-pi, pi] (fftlib.f90:1227-1228)
-          mo = std::atan2(std::sin(mo.real()), std::cos(mo.real()));
-          re = std::atan2(std::sin(re.real()), std::cos(re.real()));
+  return guarded([&]() -> int {
+    if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+    const int prec = opt && opt->precision ? opt->precision : 64;
+    if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
+    smili_batch* b = nullptr;
+    int rc = prec == 64 ? create_model<double>(*a, x, opt, &b) : create_model<float>(*a, x, opt, &b);
+    if (rc != SMILI_OK) return rc;
+    rc = run(b, MODE_FG, nullptr);
+    double terms[SMILI_NTERMS];
+    if (rc == SMILI_OK) rc = smili_batch_fetch(b, 0, nullptr, terms, grad, nullptr);
+    if (rc == SMILI_OK) {
+      const ProbDesc& d = b->descs[0];
+      std::vector<double> mr(4 * (size_t)d.ndata);
+      cudaError_t e = cudaMemcpy(mr.data(), b->d_arena + d.o_model, sizeof(double) * mr.size(), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) {
+        rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
+      } else {
+        if (chisq) *chisq = terms[0];
+        const double dix = a->nx / 2.0 + 1 - a->nxref, diy = a->ny / 2.0 + 1 - a->nyref;
+        for (int i = 0; i < d.ndata; ++i) {
+          std::complex<double> mo(mr[4 * i], mr[4 * i + 1]), re(mr[4 * i + 2], mr[4 * i + 3]);
+          if (a->isfcv) {  // phashift_c2r (fftlib.f90:200-220) of model and residual
+            const int k = std::abs(a->uvidxfcv[i]) - 1, sg = a->uvidxfcv[i] > 0 ? 1 : -1;
+            const std::complex<double> ph = std::exp(std::complex<double>(0.0, a->u[k] * sg * dix + a->v[k] * sg * diy));
+            mo *= ph;
+            re *= ph;
+          } else if (a->iscp) {  // model_cp wraps both into (-pi, pi] (fftlib.f90:1227-1228)
+            mo = std::atan2(std::sin(mo.real()), std::cos(mo.real()));
+            re = std::atan2(std::sin(re.real()), std::cos(re.real()));
+          }
+          if (model_re) model_re[i] = mo.real();
+          if (model_im) model_im[i] = mo.imag();
+          if (resid_re) resid_re[i] = re.real();
+          if (resid_im) resid_im[i] = re.imag();
         }
-        if (model_re) model_re[i] = mo.real();
-        if (model_im) model_im[i] = mo.imag();
-        if (resid_re) resid_re[i] = re.real();
-        if (resid_im) resid_im[i] = re.imag();
       }
     }
-  }
-  smili_batch_destroy(b);
-  return rc;
+    smili_batch_destroy(b);
+    return rc;
+  });
 }
 
 static smili_imaging_args bare_args(int nuv, const double* u, const double* v, int nx, int ny,
@@ -1783,60 +1821,64 @@ static smili_imaging_args bare_args(int nuv, const double* u, const double* v, i
 
 int smili_nufft_fwd_real(int nuv, const double* u, const double* v, int nx, int ny, const double* img,
                          const smili_options* opt, double* vreal, double* vimag) {
-  if (!u || !v || !img || !vreal || !vimag || nx < 1 || ny < 1 || nuv < 1)
-    return fail(SMILI_ERR_ARG, "invalid nufft arguments");
-  std::vector<double> im(img, img + (size_t)nx * ny);
-  std::vector<int> xi, yi;
-  smili_imaging_args a = bare_args(nuv, u, v, nx, ny, im, xi, yi);
-  smili_batch* b = nullptr;
-  const smili_imaging_args* probs[1] = {&a};
-  int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_T2, nullptr, nullptr, nullptr, &b);
-  if (rc != SMILI_OK) return rc;
-  // x = image in evaluation mode
-  rc = run(b, MODE_T2, nullptr);
-  if (rc == SMILI_OK) {
-    const ProbDesc& d = b->descs[0];
-    const size_t C = b->prec64 ? 16 : 8;
-    std::vector<char> buf(C * nuv);
-    cudaError_t e = cudaMemcpy(buf.data(), b->d_arena + d.o_V, C * nuv, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
-    const std::vector<int>& perm = b->perms[0];
-    for (int j = 0; j < nuv && rc == SMILI_OK; ++j) {
-      double re, im_;
-      if (b->prec64) {
-        re = reinterpret_cast<double*>(buf.data())[2 * j];
-        im_ = reinterpret_cast<double*>(buf.data())[2 * j + 1];
-      } else {
-        re = reinterpret_cast<float*>(buf.data())[2 * j];
-        im_ = reinterpret_cast<float*>(buf.data())[2 * j + 1];
+  return guarded([&]() -> int {
+    if (!u || !v || !img || !vreal || !vimag || nx < 1 || ny < 1 || nuv < 1)
+      return fail(SMILI_ERR_ARG, "invalid nufft arguments");
+    std::vector<double> im(img, img + (size_t)nx * ny);
+    std::vector<int> xi, yi;
+    smili_imaging_args a = bare_args(nuv, u, v, nx, ny, im, xi, yi);
+    smili_batch* b = nullptr;
+    const smili_imaging_args* probs[1] = {&a};
+    int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_T2, nullptr, nullptr, nullptr, &b);
+    if (rc != SMILI_OK) return rc;
+    // x = image in evaluation mode
+    rc = run(b, MODE_T2, nullptr);
+    if (rc == SMILI_OK) {
+      const ProbDesc& d = b->descs[0];
+      const size_t C = b->prec64 ? 16 : 8;
+      std::vector<char> buf(C * nuv);
+      cudaError_t e = cudaMemcpy(buf.data(), b->d_arena + d.o_V, C * nuv, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
+      const std::vector<int>& perm = b->perms[0];
+      for (int j = 0; j < nuv && rc == SMILI_OK; ++j) {
+        double re, im_;
+        if (b->prec64) {
+          re = reinterpret_cast<double*>(buf.data())[2 * j];
+          im_ = reinterpret_cast<double*>(buf.data())[2 * j + 1];
+        } else {
+          re = reinterpret_cast<float*>(buf.data())[2 * j];
+          im_ = reinterpret_cast<float*>(buf.data())[2 * j + 1];
+        }
+        vreal[perm[j]] = re;
+        vimag[perm[j]] = im_;
       }
-      vreal[perm[j]] = re;
-      vimag[perm[j]] = im_;
     }
-  }
-  smili_batch_destroy(b);
-  return rc;
+    smili_batch_destroy(b);
+    return rc;
+  });
 }
 
 int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const double* vreal, const double* vimag,
                            int nx, int ny, const smili_options* opt, double* img) {
-  if (!u || !v || !vreal || !vimag || !img || nx < 1 || ny < 1 || nuv < 1)
-    return fail(SMILI_ERR_ARG, "invalid nufft arguments");
-  std::vector<double> im;
-  std::vector<int> xi, yi;
-  smili_imaging_args a = bare_args(nuv, u, v, nx, ny, im, xi, yi);
-  smili_batch* b = nullptr;
-  const smili_imaging_args* probs[1] = {&a};
-  int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_T1, nullptr, vreal, vimag, &b);
-  if (rc != SMILI_OK) return rc;
-  rc = run(b, MODE_T1, nullptr);
-  if (rc == SMILI_OK) {
-    const ProbDesc& d = b->descs[0];
-    cudaError_t e = cudaMemcpy(img, b->d_arena + d.o_gchi, sizeof(double) * nx * ny, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
-  }
-  smili_batch_destroy(b);
-  return rc;
+  return guarded([&]() -> int {
+    if (!u || !v || !vreal || !vimag || !img || nx < 1 || ny < 1 || nuv < 1)
+      return fail(SMILI_ERR_ARG, "invalid nufft arguments");
+    std::vector<double> im;
+    std::vector<int> xi, yi;
+    smili_imaging_args a = bare_args(nuv, u, v, nx, ny, im, xi, yi);
+    smili_batch* b = nullptr;
+    const smili_imaging_args* probs[1] = {&a};
+    int rc = create_any(1, probs, nullptr, 0, 5, 1e1, 0.0, opt, PK_T1, nullptr, vreal, vimag, &b);
+    if (rc != SMILI_OK) return rc;
+    rc = run(b, MODE_T1, nullptr);
+    if (rc == SMILI_OK) {
+      const ProbDesc& d = b->descs[0];
+      cudaError_t e = cudaMemcpy(img, b->d_arena + d.o_gchi, sizeof(double) * nx * ny, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = fail(SMILI_ERR_CUDA, cudaGetErrorString(e));
+    }
+    smili_batch_destroy(b);
+    return rc;
+  });
 }
 
 }  // extern "C"
@@ -1845,8 +1887,10 @@ int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const doub
 
 extern "C" int smili_get_uvlist(int n, const double* u, const double* v, const smili_options* opt, int* nuv,
                                 double* u_out, double* v_out, int* uvidx) {
-  return uvlist_run(n, u, v, opt ? opt->device : 0, opt ? static_cast<cudaStream_t>(opt->stream) : nullptr, nuv,
-                    u_out, v_out, uvidx);
+  return guarded([&]() -> int {
+    return uvlist_run(n, u, v, opt ? opt->device : 0, opt ? static_cast<cudaStream_t>(opt->stream) : nullptr, nuv,
+                      u_out, v_out, uvidx);
+  });
 }
 
 // ===========================================================================
@@ -1984,9 +2028,11 @@ int calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_
 
 extern "C" int smili_calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_options* opt,
                                        double* terms, double* grad) {
-  if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
-  const int prec = opt && opt->precision ? opt->precision : 64;
-  if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
-  return prec == 64 ? calc_cost_noalloc<double>(a, x, opt, terms, grad)
-                    : calc_cost_noalloc<float>(a, x, opt, terms, grad);
+  return guarded([&]() -> int {
+    if (!a || !x) return fail(SMILI_ERR_ARG, "null argument");
+    const int prec = opt && opt->precision ? opt->precision : 64;
+    if (prec != 64 && prec != 32) return fail(SMILI_ERR_ARG, "precision must be 64 or 32");
+    return prec == 64 ? calc_cost_noalloc<double>(a, x, opt, terms, grad)
+                      : calc_cost_noalloc<float>(a, x, opt, terms, grad);
+  });
 }
