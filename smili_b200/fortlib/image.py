@@ -97,13 +97,54 @@ def init_tfdreg(tfd_l_in, tfd_tgtfd, tfd_tgter):
     return float(tfd_l_in) / (float(tfd_tgtfd) * float(tfd_tgter)) ** 2
 
 
-def totalflux(I1d):
-    """Sum of |I| (image.f90:1123-1136)."""
+def totalflux(I1d, N1d=None):
+    """Sum of |I| (image.f90:1125-1136).  ``N1d`` is the f2py length argument
+    (optional there too; imdata.py:1029 passes it)."""
+    I1d = np.asarray(I1d, dtype=np.float64)
+    if N1d is not None:
+        I1d = I1d[:int(N1d)]
     return float(np.sum(np.abs(I1d)))
 
 
-def xy_cen(I1d, x, y):
-    """Intensity-weighted centroid normalised by sum |I| (image.f90:1098-1121)."""
+def xy_cen(I1d, x, y, N1d=None):
+    """Intensity-weighted centroid normalised by sum |I| (image.f90:1100-1123)."""
     I1d = np.asarray(I1d, dtype=np.float64)
+    n = I1d.size if N1d is None else int(N1d)
+    I1d, x, y = I1d[:n], np.asarray(x)[:n], np.asarray(y)[:n]
     tot = np.sum(np.abs(I1d))
-    return float(np.sum(np.asarray(x) * I1d) / tot), float(np.sum(np.asarray(y) * I1d) / tot)
+    return float(np.sum(x * I1d) / tot), float(np.sum(y * I1d) / tot)
+
+
+def sigma(I1d, xidx, yidx, Isum, xcen, ycen, N1d=None):
+    """Second moments of the image about (xcen, ycen), divided by Isum:
+    [sum I (x - xc)^2, sum I (y - yc)^2, sum I (x - xc)(y - yc)] / Isum
+    (``Sigma``, image.f90:1039-1053; imdata.py:1031 calls it as sigma)."""
+    I1d = np.asarray(I1d, dtype=np.float64)
+    n = I1d.size if N1d is None else int(N1d)
+    I1d = I1d[:n]
+    dx = np.asarray(xidx, dtype=np.float64)[:n] - xcen
+    dy = np.asarray(yidx, dtype=np.float64)[:n] - ycen
+    return np.array([np.sum(I1d * dx ** 2 / Isum), np.sum(I1d * dy ** 2 / Isum), np.sum(I1d * dx * dy / Isum)])
+
+
+# check_sm_character's pi is the single-precision literal 3.1415926535
+# widened to double (image.f90:1062), kept for parity
+_PI_SM = float(np.float32(3.1415926535))
+
+
+def check_sm_character(Sg):
+    """Major / minor second moments and the position angle of the ellipse
+    with second-moment matrix [[Sg1, Sg3], [Sg3, Sg2]] (image.f90:1055-1078):
+    returns (maj, min, phi), phi measured from the RA axis."""
+    s1, s2, s3 = (float(v) for v in np.asarray(Sg, dtype=np.float64)[:3])
+    root = np.sqrt(4.0 * s3 ** 2 + (s1 - s2) ** 2) / 2.0
+    mj = (s1 + s2) / 2.0 + root
+    mn = (s1 + s2) / 2.0 - root
+    with np.errstate(invalid="ignore", divide="ignore"):
+        phi = float(np.arcsin(2.0 * s3 / (mj - mn)) / 2.0)
+    if s1 / s2 > 1.0:
+        if s3 > 0.0:
+            phi = 0.5 * _PI_SM - phi
+        if s3 < 0.0:
+            phi = -0.5 * _PI_SM - phi
+    return mj, mn, -phi

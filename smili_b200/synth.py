@@ -179,16 +179,9 @@ def random_stations(rng: np.random.Generator, n: int) -> np.ndarray:
 
 
 def calc_uvw(gst_hour, alpha, delta, bx, by, bz):
-    """Baseline vector -> (u, v, w), restating src/fortlib/coord.f90:37-59."""
-    gh = gst_hour * np.pi / 12 - alpha
-    cosgh, singh = np.cos(gh), np.sin(gh)
-    blx = cosgh * bx - singh * by
-    bly = singh * bx + cosgh * by
-    blz = bz
-    u = bly
-    v = -blx * np.sin(delta) + blz * np.cos(delta)
-    w = blx * np.cos(delta) + blz * np.sin(delta)
-    return u, v, w
+    """Baseline vector -> (u, v, w) (``fortlib.coord.calc_uvw``)."""
+    from .fortlib.coord import calc_uvw as _calc_uvw
+    return _calc_uvw(gst_hour, alpha, delta, bx, by, bz)
 
 
 def exact_dft(img_data: np.ndarray, img: Image, u: np.ndarray, v: np.ndarray,
