@@ -135,13 +135,22 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
     totalflux_scaled = totalflux * inormfactr
 
     def prior_array(prior):
+        # The reference takes the prior's pixels as a view of prior.data when
+        # there is no window (lbfgs.py:275, 298, 328, 357, 380) and then
+        # normalises it in place, so a prior image shared by several
+        # regularizers reaches the later ones already normalised (and the
+        # caller's image is changed).  Kept for identical weights.
         if imregion is None:
-            return np.array(prior.data[0, 0], dtype=np.float64).reshape(Nyx)
-        return np.array(prior.data[0, 0], dtype=np.float64)[winidx]
+            return prior.data[0, 0].reshape(Nyx)
+        return prior.data[0, 0][winidx]
+
+    # A 0-d float64, as np.float64(np.asarray([0])) gives in the reference
+    # (lbfgs.py:265, 287, 317, 347, 370); f2py broadcasts it to length 1.
+    zero = np.float64(0.0)
 
     # regularizers (lbfgs.py:264-414)
     if l1_lambda <= 0:
-        l1_wgt, l1_nwgt, l1_l = np.float64([0]), 1, -1
+        l1_wgt, l1_nwgt, l1_l = zero, 1, -1
     else:
         if l1_prior is None:
             pr = np.full(Npix, totalflux_scaled / Npix)
@@ -153,7 +162,7 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
         l1_wgt = fortlib.image.init_l1reg(pr)
         l1_nwgt, l1_l = len(l1_wgt), l1_lambda
     if tv_lambda <= 0:
-        tv_wgt, tv_nwgt, tv_l = np.float64([0]), 1, -1
+        tv_wgt, tv_nwgt, tv_l = zero, 1, -1
     else:
         if tv_prior is None:
             pr, flat = np.full(Npix, totalflux_scaled / Npix), True
@@ -164,7 +173,7 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
                                           tv_prior=pr)
         tv_nwgt, tv_l = len(tv_wgt), tv_lambda
     if tsv_lambda <= 0:
-        tsv_wgt, tsv_nwgt, tsv_l = np.float64([0]), 1, -1
+        tsv_wgt, tsv_nwgt, tsv_l = zero, 1, -1
     else:
         if tsv_prior is None:
             pr, flat = np.full(Npix, totalflux_scaled / Npix), True
@@ -175,14 +184,14 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
                                             tsv_isflat=flat, tsv_prior=pr)
         tsv_nwgt, tsv_l = len(tsv_wgt), tsv_lambda
     if kl_lambda <= 0:
-        kl_wgt, kl_nwgt, kl_l = np.float64([0]), 1, -1
+        kl_wgt, kl_nwgt, kl_l = zero, 1, -1
     else:
         pr = np.full(Npix, totalflux_scaled / Npix) if kl_prior is None else prior_array(kl_prior)
         pr *= totalflux_scaled / pr.sum()
         kl_l, kl_wgt = fortlib.image.init_klreg(kl_l_in=kl_lambda, kl_prior=pr)
         kl_nwgt = len(kl_wgt)
     if gs_lambda <= 0:
-        gs_wgt, gs_nwgt, gs_l = np.float64([0]), 1, -1
+        gs_wgt, gs_nwgt, gs_l = zero, 1, -1
     else:
         pr = np.full(Npix, totalflux_scaled / Npix) if gs_prior is None else prior_array(gs_prior)
         pr *= totalflux_scaled / pr.sum()
@@ -207,7 +216,7 @@ def prepare_imaging(initimage, imregion=None, vistable=None, amptable=None, bsta
         sm_min = (sm_min / dtheta) ** 2 / (8. * np.log(2.))
         sm_phi = -sm_phi / 180. * np.pi
 
-    dummy = np.float64([0.])
+    dummy = zero  # dammyreal, lbfgs.py:425
     conv = getattr(initimage, "angconv", None)
     if vistable is None:  # lbfgs.py:421-480
         isfcv, vfcvr, vfcvi, varfcv = False, dummy, dummy, dummy

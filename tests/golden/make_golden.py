@@ -10,6 +10,8 @@ Usage (in a container that has the reference checkout)::
 
     python tests/golden/make_golden.py /path/to/reference
 
+or with $SMILI_REFERENCE_ROOT set and no argument.
+
 writes ``tests/golden/uvlist_*.npz`` (inputs and reference outputs).
 """
 from __future__ import annotations
@@ -91,4 +93,7 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SMILI_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("usage: make_golden.py REFERENCE_ROOT (or set $SMILI_REFERENCE_ROOT)")
+    main(root)

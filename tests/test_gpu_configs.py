@@ -1,0 +1,140 @@
+"""CUDA path against the CPU oracle at the benchmark's own problem sizes.
+
+The 256x256 precision-path workload (1 uas pixels, 10 stations, 97 200
+visibilities with station gains, amplitudes with 5 % error + 77 760 closure
+phases + 75 600 log closure amplitudes, l1 / TV / MEM = 1 / 1 / 0.1; the
+chi-square path of fftlib.f90:250-655 and the regularizers of
+image.f90:12-200) and the 64x64 crescent workload (8 stations, 2 016 complex
+visibilities + 1 512 closure phases, l1 = tsv = 1, 20 uas Gaussian prior;
+the L-BFGS-B loop of fftim2d.f90:286-351).
+
+Inputs come from the exact DFT on the host (no device code is involved in
+making them).  Tolerances:
+
+- FP64, NUFFT tolerance 1e-12 on both sides: every cost term within 1e-9
+  relative, the gradient within 1e-8 relative (max-norm).
+- FP64 at the reference's own tolerance 1e-6 (wrapfinufft.f90:8) on both
+  sides: the same kernel width, shape parameter, fine grid and deconvolution
+  rule, so the two evaluations differ by rounding only: 1e-10 on the
+  objective, 1e-9 on the gradient.
+- FP32 (NUFFT tolerance 1e-6, compensated chi-square sums) against the exact
+  FP64 oracle: the objective within 1e-4 relative, the gradient no further
+  from it than twice the FP64 oracle's own error at tolerance 1e-6, plus 1e-4.
+- L-BFGS-B per iteration (FP64): the first 10 iterations within 1e-9
+  relative (1e-7 with closure terms), the first 50 within 2e-5.
+"""
+import numpy as np
+import pytest
+
+from conftest import make_kw
+
+pytestmark = pytest.mark.gpu
+
+TERMS = ["cost", "chisq", "reg", "chisqfcv", "chisqamp", "chisqcp", "chisqca", "l1_cost",
+         "tv_cost", "tsv_cost", "kl_cost", "gs_cost", "tfd_cost", "cen_cost", "sm_cost"]
+
+
+def _rel(a, b):
+    return np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(np.asarray(b)).max(), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def cfg2():
+    """The 256x256 / 97 200-visibility workload (first seed of the benchmark)."""
+    from smili_b200 import synth
+    obs = synth.precision_path(seed=1000, niter=1000)
+    kw = make_kw(obs)
+    assert kw["nx"] == 256 and np.size(kw["uvidxamp"]) == 97200
+    assert np.shape(kw["uvidxcp"])[1] == 77760 and np.shape(kw["uvidxca"])[1] == 75600
+    return obs, kw
+
+
+@pytest.fixture(scope="module")
+def cfg1():
+    """The 64x64 crescent workload."""
+    from smili_b200 import synth
+    obs = synth.small_crescent(seed=0, nx=64, niter=1000)
+    kw = make_kw(obs)
+    assert kw["nx"] == 64 and np.size(kw["uvidxfcv"]) == 2016 and np.shape(kw["uvidxcp"])[1] == 1512
+    return obs, kw
+
+
+def _points(obs, kw):
+    """Evaluation points: the prior with 30 % pixel noise, and the truth
+    (a structured image) in the solver's normalised units."""
+    rng = np.random.default_rng(11)
+    x0 = kw["iin"] * (1 + 0.3 * rng.random(kw["iin"].size))
+    truth = np.asarray(obs.truth)[np.asarray(kw["yidx"]) - 1, np.asarray(kw["xidx"]) - 1]
+    return {"prior": x0, "truth": truth * float(kw["inormfactr"])}
+
+
+@pytest.mark.parametrize("point", ["prior", "truth"])
+def test_cfg2_fp64_matches_oracle(oracle, cfg2, point):
+    from smili_b200.fortlib import fftim2d
+    obs, kw = cfg2
+    x = _points(obs, kw)[point]
+    t_ref, g_ref = oracle.calc_cost(kw, x, eps=1e-12)
+    t_gpu, g_gpu = fftim2d.calc_cost(x, nufft_eps=1e-12, **kw)
+    for k in TERMS:
+        assert abs(t_gpu[k] - t_ref[k]) <= 1e-9 * max(abs(t_ref[k]), 1e-12), (k, t_gpu[k], t_ref[k])
+    assert _rel(g_gpu, g_ref) < 1e-8
+
+
+@pytest.mark.parametrize("point", ["prior", "truth"])
+def test_cfg2_fp64_eps6_matches_oracle_to_rounding(oracle, cfg2, point):
+    from smili_b200.fortlib import fftim2d
+    obs, kw = cfg2
+    x = _points(obs, kw)[point]
+    t_ref, g_ref = oracle.calc_cost(kw, x, eps=1e-6)
+    t_gpu, g_gpu = fftim2d.calc_cost(x, nufft_eps=1e-6, **kw)
+    for k in TERMS:
+        assert abs(t_gpu[k] - t_ref[k]) <= 1e-10 * max(abs(t_ref[k]), 1e-12), (k, t_gpu[k], t_ref[k])
+    assert _rel(g_gpu, g_ref) < 1e-9
+
+
+@pytest.mark.parametrize("point", ["prior", "truth"])
+def test_cfg2_fp32_bound(oracle, cfg2, point):
+    from smili_b200.fortlib import fftim2d
+    obs, kw = cfg2
+    x = _points(obs, kw)[point]
+    t_ref, g_ref = oracle.calc_cost(kw, x, eps=1e-12)
+    _, g_ref6 = oracle.calc_cost(kw, x, eps=1e-6)
+    t32, g32 = fftim2d.calc_cost(x, precision=32, nufft_eps=1e-6, **kw)
+    for k in ("cost", "chisq", "chisqamp", "chisqcp", "chisqca", "reg"):
+        assert abs(t32[k] - t_ref[k]) <= 1e-4 * abs(t_ref[k]), (k, t32[k], t_ref[k])
+    assert _rel(g32, g_ref) <= 2.0 * _rel(g_ref6, g_ref) + 1e-4
+
+
+def test_cfg2_solve_first_iterations_match_oracle(oracle, cfg2):
+    """Ten L-BFGS-B iterations of the 256x256 workload from its 60 uas prior (FP64)."""
+    from smili_b200 import _lib
+    obs, kw = cfg2
+    k = dict(kw, niter=10)
+    b = _lib.Batch([_lib.Problem(k)], niter=10, options=_lib.make_options(64, 1e-12))
+    b.run()
+    _, _, _, info = b.fetch(0)
+    tr = b.trace(0, 12)
+    b.close()
+    _, _, iref = oracle.imaging(k, eps=1e-12)
+    assert info["niter"] == iref["niter"]
+    np.testing.assert_allclose(tr[:10], iref["trace"][:10], rtol=1e-7)
+
+
+@pytest.mark.parametrize("eps", [1e-12, 1e-6])
+def test_cfg1_solve_50_iterations_match_oracle(oracle, cfg1, eps):
+    """Fifty L-BFGS-B iterations of the 64x64 crescent workload from the
+    20 uas prior, per iteration (FP64), at a tight NUFFT tolerance and at the
+    reference's own (the drop-in's default path)."""
+    from smili_b200 import _lib
+    obs, kw = cfg1
+    k = dict(kw, niter=50)
+    b = _lib.Batch([_lib.Problem(k)], niter=50, options=_lib.make_options(64, eps))
+    b.run()
+    _, terms, _, info = b.fetch(0)
+    tr = b.trace(0, 52)
+    b.close()
+    _, tref, iref = oracle.imaging(k, eps=eps)
+    assert info["niter"] == iref["niter"] == 51
+    np.testing.assert_allclose(tr[:10], iref["trace"][:10], rtol=1e-9)
+    np.testing.assert_allclose(tr[:50], iref["trace"][:50], rtol=2e-5)
+    assert abs(terms["cost"] - tref["cost"]) <= 1e-4 * abs(tref["cost"])

@@ -10,7 +10,10 @@ import pytest
 
 from conftest import make_kw
 
-EXAMPLES = "/root/reference/docs/examples/uvdata"
+from reference_dropin import reference_root
+
+# the reference's example tables, when $SMILI_REFERENCE_ROOT names a checkout
+EXAMPLES = os.path.join(reference_root() or "", "docs", "examples", "uvdata")
 
 
 def _roundtrip(tab, reader, tmp_path, name):
