@@ -220,17 +220,21 @@ int smili_nufft_adj_real1d(int nuv, const double* u, const double* v, const doub
                            double* img);
 
 /* Allocation-free calc_cost (no reference counterpart).  Same inputs,
- * outputs and results as smili_calc_cost, for callers that must not
- * allocate device memory (e.g. a host whose device memory is owned by
- * another allocator or pool, or code that runs between the launches of a
- * captured stream).  Its device scratch is one static array of
+ * outputs and results as smili_calc_cost (the same options: precision,
+ * NUFFT tolerance, CTAs per problem, spreading tile, transform), for
+ * callers that must not allocate device memory, e.g. a host whose device
+ * memory is owned by another allocator or pool that leaves no room for
+ * cudaMalloc.  Its device scratch is one static array of
  * SMILI_NOALLOC_SCRATCH_BYTES per device: problems that need more are
  * rejected with SMILI_ERR_ARG (use smili_calc_cost for those).  It calls no
  * CUDA allocator; host-side packing uses ordinary host memory.  Calls on
- * the same device share the scratch, so calls that overlap in time race;
- * the first call on a device does the set-up (cudaGetSymbolAddress and
- * kernel attributes) and should come before any stream capture.  Runs on
- * opt->stream, or the per-thread default stream when that is NULL. */
+ * the same device share the scratch, so calls that overlap in time race.
+ * The first call on a device does the set-up (cudaGetSymbolAddress and
+ * kernel attributes), kept for the life of the process: a cudaDeviceReset
+ * after it is not supported.  The call is synchronous (it waits for its
+ * stream and reads the results back with blocking copies): do not make it
+ * while any stream of the process is capturing.  Runs on opt->stream, or
+ * the per-thread default stream when that is NULL. */
 #define SMILI_NOALLOC_SCRATCH_BYTES (16u << 20)
 int smili_calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_options* opt,
                             double* terms, double* grad);

@@ -1904,7 +1904,11 @@ extern "C" int smili_get_uvlist(int n, const double* u, const double* v, const s
 // fit are rejected with SMILI_ERR_ARG.  The one scratch array is shared by
 // all calls on a device, so calls that overlap in time (other threads or
 // streams) race; the first call on a device performs the set-up and should
-// come before any stream capture.
+// come before any stream capture.  The call is synchronous (it waits for its
+// stream and copies the results back with blocking copies), so it must not
+// be made while any stream of the process is capturing.  The set-up is kept
+// for the life of the process: a cudaDeviceReset after the first call on a
+// device is not supported.
 // ===========================================================================
 #include <mutex>
 
@@ -1948,7 +1952,9 @@ int calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_
   if (!(eps < 1.0)) return fail(SMILI_ERR_ARG, "nufft_eps must be in (0, 1)");
   Arena ar;
   HostProb hp;
-  int rc = pack_problem<R>(*a, PK_FG, 0, 0, 5, 1e1, 0.0, eps, ar, hp, x, nullptr, nullptr);
+  ar.take(256);  // as create_batch: no present field at offset 0, the mark of an absent one
+  int rc = pack_problem<R>(*a, PK_FG, 0, 0, 5, 1e1, 0.0, eps, ar, hp, x, nullptr, nullptr, 0.0,
+                           opt && opt->spread_bin ? opt->spread_bin : 8, opt ? opt->transform : 0);
   if (rc != SMILI_OK) return rc;
   const size_t arena_al = round256(std::max<size_t>(ar.bytes, 256));
   if (arena_al > kNoAllocBytes)
@@ -1977,7 +1983,10 @@ int calc_cost_noalloc(const smili_imaging_args* a, const double* x, const smili_
   if (!coop || occ < 1) return fail(SMILI_ERR_CUDA, "cooperative launch unavailable");
   const int maxres = occ * nsm;
   int G = opt && opt->ctas_per_problem > 0 ? opt->ctas_per_problem : 0;
-  if (G <= 0) G = std::max(1, std::min(maxres, (hp.d.npix + 1023) / 1024));
+  if (G <= 0) {  // finish_batch's rule for one problem: about four pixels per thread
+    const int per_cta = 4 * Shape<R>::threads;
+    G = std::max(1, std::min(maxres, (hp.d.npix + per_cta - 1) / per_cta));
+  }
   G = std::min(G, maxres);
   b.G = G;
   b.ngroups = 1;

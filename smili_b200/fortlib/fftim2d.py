@@ -32,10 +32,12 @@ def imaging(precision=64, nufft_eps=0.0, ctas_per_problem=0, device=0, info=None
     return (iout,) + tuple(float(t) for t in terms)
 
 
-def calc_cost(x, precision=64, nufft_eps=0.0, device=0, **kw):
-    """calc_cost (fftim2d.f90:387-607) at image vector x: (terms dict, grad)."""
+def calc_cost(x, precision=64, nufft_eps=0.0, device=0, spread_bin=0, transform=0, **kw):
+    """calc_cost (fftim2d.f90:387-607) at image vector x: (terms dict, grad).
+    ``spread_bin`` (8 | 16) and ``transform`` (0 automatic, 1 radix passes,
+    2 dense band products) select the launch's spreading tile and band path."""
     prob = _lib.Problem(kw)
-    opt = _lib.make_options(precision, nufft_eps, 0, device)
+    opt = _lib.make_options(precision, nufft_eps, 0, device, spread_bin=spread_bin, transform=transform)
     x = np.ascontiguousarray(x, dtype=np.float64)
     terms = np.zeros(15)
     grad = np.zeros(prob.npix)
@@ -44,13 +46,14 @@ def calc_cost(x, precision=64, nufft_eps=0.0, device=0, **kw):
     return dict(zip(_lib.TERM_NAMES, terms)), grad
 
 
-def calc_cost_noalloc(x, precision=64, nufft_eps=0.0, device=0, **kw):
+def calc_cost_noalloc(x, precision=64, nufft_eps=0.0, device=0, spread_bin=0, transform=0, **kw):
     """calc_cost through the allocation-free entry point: the same result as
-    ``calc_cost`` for problems whose device arena fits the library's static
-    scratch (others raise SmiliError with code -1).  Calls on one device
-    must not overlap."""
+    ``calc_cost`` (same options) for problems whose device arena fits the
+    library's static scratch (others raise SmiliError with code -1).  Calls
+    on one device must not overlap, and none may be made while a stream is
+    capturing (the call is synchronous)."""
     prob = _lib.Problem(kw)
-    opt = _lib.make_options(precision, nufft_eps, 0, device)
+    opt = _lib.make_options(precision, nufft_eps, 0, device, spread_bin=spread_bin, transform=transform)
     x = np.ascontiguousarray(x, dtype=np.float64)
     terms = np.zeros(15)
     grad = np.zeros(prob.npix)

@@ -47,6 +47,22 @@ def test_noalloc_matches_calc_cost(problem, precision, eps, rtol):
     assert _close(g_na, first[1], rtol)
 
 
+@pytest.mark.parametrize("spread_bin,transform", [(16, 0), (8, 1), (8, 2)])
+def test_noalloc_honours_launch_options(problem, spread_bin, transform):
+    """The spreading tile and band path of the options reach the
+    allocation-free call as they reach smili_calc_cost (FP64 at the
+    reference's NUFFT tolerance: the same sums, rounding only)."""
+    from smili_b200.fortlib import fftim2d
+    kw, x1, x2 = problem
+    for x in (x1, x2):
+        t_ref, g_ref = fftim2d.calc_cost(x, precision=64, nufft_eps=1e-6, spread_bin=spread_bin,
+                                         transform=transform, **kw)
+        t_na, g_na = fftim2d.calc_cost_noalloc(x, precision=64, nufft_eps=1e-6, spread_bin=spread_bin,
+                                               transform=transform, **kw)
+        assert abs(t_na["cost"] - t_ref["cost"]) <= 1e-11 * abs(t_ref["cost"])
+        assert _close(g_na, g_ref, 1e-11)
+
+
 def test_noalloc_rejects_oversize():
     from smili_b200 import _lib, synth
     from smili_b200.fortlib import fftim2d
