@@ -22,7 +22,10 @@ extern "C" {
 #define SMILI_UNET_ERR_CUDA (-3)
 
 /* y (+)= act(conv3x3(x, w) + bias): pad 1, stride 1, FP32 accumulation on the
- * tensor cores.  relu != 0 applies max(0, .); accumulate != 0 adds to y. */
+ * tensor cores.  relu != 0 applies max(0, .); accumulate != 0 adds to y.
+ * When Cin and ldx are multiples of 8 and x, w are 16-byte aligned, the
+ * convolution runs on the tcgen05 tensor cores (TMA-staged operands, FP32
+ * accumulator in tensor memory); otherwise on mma.sync. */
 int smili_unet_conv3x3(const void* x, int N, int H, int W, int Cin, int ldx, const void* w, const float* bias,
                        void* y, int ldy, int Cout, int relu, int accumulate, void* stream);
 
@@ -63,6 +66,19 @@ int smili_unet_adam(float* w, void* w16, const float* g, float* m, float* v, lon
                     float b2, float eps, float wd, int step, void* stream);
 
 int smili_unet_f32_to_bf16(const float* x, void* y, long long n, void* stream);
+
+/* Convolution path: 0 (default) tcgen05 where it applies, 1 mma.sync always.
+ * Process-wide; for comparisons and tests. */
+int smili_unet_set_conv_path(int path);
+
+/* Reads and clears the tcgen05 convolution's error flag (synchronous):
+ * 0, or the code of a bounded wait inside the kernel that ran out (1 stage
+ * release, 2 operand arrival, 3 accumulator completion, 4 outstanding copy),
+ * or SMILI_UNET_ERR_CUDA. */
+int smili_unet_tc_status(void);
+
+/* Why the last tcgen05 convolution call of this thread failed ("" if none). */
+const char* smili_unet_last_error(void);
 
 #ifdef __cplusplus
 }

@@ -18,7 +18,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 LIBS = {
     "libsmili_b200.so": ("solver.cu", ["common.cuh", "fft.cuh", "fg.cuh", "lbfgsb.cuh", "layout.h", "uvlist.cuh"],
                          ["smili_b200.h"]),
-    "libsmili_unet.so": ("unet.cu", [], ["smili_unet.h"]),
+    "libsmili_unet.so": ("unet.cu", ["conv_tc.cuh"], ["smili_unet.h"]),
 }
 
 OUT = os.path.join(HERE, "libsmili_b200.so")

@@ -15,11 +15,18 @@
 // The data gradient is the same kernel on the ReLU-masked output gradient
 // with flipped, transposed weights; the weight gradient is a second
 // implicit GEMM over pixels with deterministic per-split partial sums.
+// Convolutions whose input rows and weights TMA can address (Cin and the
+// channel stride multiples of 8, 16-byte aligned bases) run instead on the
+// tcgen05 tensor cores with the accumulator in tensor memory (conv_tc.cuh);
+// the mma.sync kernel below takes the rest (the one-channel input layer).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "../../include/smili_unet.h"
+#include "conv_tc.cuh"
 
 namespace {
 
@@ -409,6 +416,9 @@ __global__ void f32_to_bf16_kernel(const float* x, __nv_bfloat16* y, size_t n) {
     y[i] = __float2bfloat16(x[i]);
 }
 
+// 0: tensor-core (tcgen05) path where it applies, else mma.sync; 1: always mma.sync
+int g_conv_path = 0;
+
 int grid_for(size_t n, int block = 256) {
   size_t g = (n + block - 1) / block;
   if (g > 148 * 32) g = 148 * 32;
@@ -447,6 +457,10 @@ int smili_unet_conv3x3(const void* x, int N, int H, int W, int Cin, int ldx, con
   const long long tiles = (long long)a.tiles_x * a.tiles_y * N;
   if (tiles > 0x7fffffffLL) return SMILI_UNET_ERR_ARG;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g_conv_path != 1 && tc::eligible(x, Cin, ldx, w, Cout))
+    return tc::launch(a.x, N, H, W, Cin, ldx, a.w, bias, a.y, ldy, Cout, relu, accumulate, s) == 0
+               ? 0
+               : SMILI_UNET_ERR_CUDA;
   if (Cout <= 8) {
     conv3x3_kernel<1><<<dim3((unsigned)tiles, 1), 256, 0, s>>>(a);
   } else if (Cout <= 16) {
@@ -556,6 +570,24 @@ int smili_unet_adam(float* w, void* w16, const float* g, float* m, float* v, lon
   adam_kernel<<<grid_for((size_t)n), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       w, static_cast<__nv_bfloat16*>(w16), g, m, v, (size_t)n, lr, b1, b2, eps, wd, bc1, bc2);
   return check_launch();
+}
+
+int smili_unet_set_conv_path(int path) {
+  if (path < 0 || path > 1) return SMILI_UNET_ERR_ARG;
+  g_conv_path = path;
+  return 0;
+}
+
+const char* smili_unet_last_error(void) { return tc::last_error().c_str(); }
+
+int smili_unet_tc_status(void) {
+  int e = 0;
+  if (cudaMemcpyFromSymbol(&e, tc::g_tc_err, sizeof(int)) != cudaSuccess) return SMILI_UNET_ERR_CUDA;
+  if (e) {
+    const int zero = 0;
+    if (cudaMemcpyToSymbol(tc::g_tc_err, &zero, sizeof(int)) != cudaSuccess) return SMILI_UNET_ERR_CUDA;
+  }
+  return e;
 }
 
 int smili_unet_f32_to_bf16(const float* x, void* y, long long n, void* stream) {

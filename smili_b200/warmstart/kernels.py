@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(HERE, "libsmili_unet.so")
 
 EXPORTS = ["smili_unet_conv3x3", "smili_unet_conv3x3_wgrad", "smili_unet_bias_grad", "smili_unet_flip_weights",
            "smili_unet_relu_mask", "smili_unet_avgpool2", "smili_unet_avgpool2_bwd", "smili_unet_upsample2",
-           "smili_unet_upsample2_bwd", "smili_unet_mse", "smili_unet_adam", "smili_unet_f32_to_bf16"]
+           "smili_unet_upsample2_bwd", "smili_unet_mse", "smili_unet_adam", "smili_unet_f32_to_bf16",
+           "smili_unet_set_conv_path", "smili_unet_tc_status", "smili_unet_last_error"]
 
 _lib = None
 
@@ -39,11 +40,15 @@ def lib():
             "smili_unet_mse": [vp, i, vp, ll, vp, i, vp, i, vp],
             "smili_unet_adam": [vp, vp, vp, vp, vp, ll, f, f, f, f, f, i, vp],
             "smili_unet_f32_to_bf16": [vp, vp, ll, vp],
+            "smili_unet_set_conv_path": [i],
+            "smili_unet_tc_status": [],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = C.c_int
+        L.smili_unet_last_error.argtypes = []
+        L.smili_unet_last_error.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -65,7 +70,8 @@ def _stream():
 
 def _check(rc, name):
     if rc != 0:
-        raise RuntimeError(f"{name} failed with status {rc}")
+        why = (lib().smili_unet_last_error() or b"").decode()
+        raise RuntimeError(f"{name} failed with status {rc}" + (f": {why}" if why else ""))
 
 
 def conv3x3(x, N, H, W, Cin, ldx, w, bias, y, ldy, Cout, relu, accumulate=False):
@@ -119,3 +125,13 @@ def adam(w, w16, g, m, v, n, lr, b1, b2, eps, wd, step):
 
 def f32_to_bf16(x, y, n):
     _check(lib().smili_unet_f32_to_bf16(_p(x), _p(y), n, _stream()), "f32_to_bf16")
+
+
+def set_conv_path(path):
+    """0: tcgen05 convolutions where they apply (default); 1: mma.sync always."""
+    _check(lib().smili_unet_set_conv_path(int(path)), "set_conv_path")
+
+
+def tc_status():
+    """Read and clear the tcgen05 convolution's error flag (0: no bounded wait ran out)."""
+    return int(lib().smili_unet_tc_status())

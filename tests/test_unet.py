@@ -122,6 +122,39 @@ def test_conv3x3_channel_slices():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("N,H,W,Cin,Cout", [(4, 128, 128, 24, 24), (4, 64, 64, 48, 48), (4, 32, 32, 96, 96),
+                                            (4, 16, 16, 192, 192), (4, 32, 32, 288, 96), (2, 24, 40, 48, 300),
+                                            (1, 8, 8, 16, 8)])
+def test_conv3x3_tcgen05_matches_mma_sync(N, H, W, Cin, Cout):
+    """The tcgen05 path (TMA-staged operands, accumulator in tensor memory)
+    against the mma.sync path and the oracle on the U-Net's layer shapes,
+    two output-channel tiles (Cout 300) and a ragged image (24 x 40); no
+    bounded wait inside the kernel runs out."""
+    import torch
+    from smili_b200.warmstart import kernels as K
+    rng = np.random.default_rng(H * 7 + Cin)
+    x = U.bf16(rng.standard_normal((N, H, W, Cin)))
+    w = U.bf16(rng.standard_normal((Cout, 3, 3, Cin)) / np.sqrt(9 * Cin))
+    b = rng.standard_normal(Cout).astype(np.float32)
+    xt, wt, bt = _bf16_tensor(x), _bf16_tensor(w), torch.as_tensor(b).cuda()
+    outs = []
+    try:
+        for path in (0, 1):
+            K.set_conv_path(path)
+            y = torch.zeros((N, H, W, Cout), dtype=torch.bfloat16, device="cuda")
+            K.conv3x3(xt, N, H, W, Cin, Cin, wt, bt, y, Cout, Cout, True)
+            torch.cuda.synchronize()
+            outs.append(_np(y))
+    finally:
+        K.set_conv_path(0)
+    assert K.tc_status() == 0
+    want = U.conv3x3(x, w, b, True)
+    # both accumulate the same products in FP32 (in another order) and round once to bf16
+    assert _close_bf16(outs[0], want)
+    assert _close_bf16(outs[1], want)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("N,H,W,Cin,Cout", [(2, 16, 16, 1, 24), (2, 32, 32, 24, 24), (1, 16, 16, 288, 96),
                                             (2, 8, 8, 96, 192), (1, 12, 20, 20, 1)])
 def test_conv3x3_wgrad_kernel(N, H, W, Cin, Cout):
