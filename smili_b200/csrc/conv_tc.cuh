@@ -245,10 +245,33 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
   const int oy = y0 + r / TILE_W, ox = x0 + r % TILE_W;
   const bool in = oy < p.H && ox < p.W;
   __nv_bfloat16* dst = p.y + (((size_t)n * p.H + (in ? oy : 0)) * p.W + (in ? ox : 0)) * p.ldy;
+  // 16-byte stores when the row of output channels allows them
+  const bool vec = (p.ldy % 8 == 0) && ((reinterpret_cast<uintptr_t>(p.y) & 15) == 0) && ((co0 & 7) == 0);
   for (int c = 0; c < p.ntile; c += 16) {
     float v[16];
     tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
     if (!in) continue;
+    if (vec && co0 + c + 16 <= p.Cout) {
+      uint4 old[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+      if (p.accumulate) {
+        old[0] = *reinterpret_cast<const uint4*>(dst + co0 + c);
+        old[1] = *reinterpret_cast<const uint4*>(dst + co0 + c + 8);
+      }
+      const __nv_bfloat16* ob = reinterpret_cast<const __nv_bfloat16*>(old);
+      uint4 out[2];
+      __nv_bfloat16* o = reinterpret_cast<__nv_bfloat16*>(out);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        float x = v[i];
+        if (p.bias) x += __ldg(p.bias + co0 + c + i);
+        if (p.relu) x = fmaxf(x, 0.f);
+        if (p.accumulate) x += __bfloat162float(ob[i]);
+        o[i] = __float2bfloat16(x);
+      }
+      *reinterpret_cast<uint4*>(dst + co0 + c) = out[0];
+      *reinterpret_cast<uint4*>(dst + co0 + c + 8) = out[1];
+      continue;
+    }
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int co = co0 + c + i;
