@@ -502,6 +502,72 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def profile_case(case, device=0):
+    """One small launch of interest for an ncu capture (``--case``):
+
+    - ``traffic``: the benchmark's concurrency (74 resident groups of 4 CTAs,
+      74 problems of the workload) for 20 FP32 iterations;
+    - ``fg``: one FP32 function/gradient evaluation of those 74 problems;
+    - ``t2`` / ``t1``: one FP32 type-2 / type-1 transform of the workload's
+      97 200 uv points on the 256 x 256 grid (the transform stages alone);
+    - ``conv``: the U-Net convolution 32 x 64 x 64, 192 -> 192 channels,
+      timed with CUDA events on the tcgen05 path and the mma.sync path.
+
+    Inputs come from the library's own transform (fast), not the exact DFT."""
+    from smili_b200 import _lib, synth
+    from smili_b200.imaging.lbfgs import prepare_imaging
+    if case in ("traffic", "fg", "t2", "t1"):
+        kws = []
+        for s in range(16 if case in ("traffic", "fg") else 1):
+            obs = synth.precision_path(seed=1000 + s, niter=20, model=synth.nufft_model)
+            kw, _ = prepare_imaging(obs.image, amptable=obs.amptable, bstable=obs.bstable,
+                                    catable=obs.catable, niter=20, **obs.reg)
+            kws.append(kw)
+    if case in ("traffic", "fg"):
+        P = [_lib.Problem(k) for k in kws]
+        b = _lib.Batch([P[i % 16] for i in range(74)], niter=20 if case == "traffic" else 1,
+                       options=_lib.make_options(32, 1e-6, 4, device))
+        ms = b.run(fg_only=case == "fg")
+        nfg = sum(b.fetch(p)[3]["nfg"] for p in range(74))
+        b.close()
+        print(json.dumps({"case": case, "ms": ms, "evaluations": nfg}))
+    elif case in ("t2", "t1"):
+        from smili_b200.fortlib import fftlib
+        u, v = np.asarray(kws[0]["u"]), np.asarray(kws[0]["v"])
+        rng = np.random.default_rng(0)
+        if case == "t2":
+            fftlib.nufft_fwd_real(u, v, rng.random((256, 256)), precision=32, nufft_eps=1e-6, device=device)
+        else:
+            c = rng.standard_normal(u.size)
+            fftlib.nufft_adj_real1d(u, v, c, np.zeros_like(c), 256, 256, precision=32, nufft_eps=1e-6,
+                                    device=device)
+        print(json.dumps({"case": case, "uv_points": int(u.size)}))
+    elif case == "conv":
+        import torch
+        from smili_b200.warmstart import kernels as K
+        N, H, W, C = 32, 64, 64, 192
+        x = torch.randn(N, H, W, C, device=f"cuda:{device}").to(torch.bfloat16)
+        w = (torch.randn(C, 3, 3, C, device=f"cuda:{device}") / 20).to(torch.bfloat16)
+        y = torch.zeros(N, H, W, C, device=f"cuda:{device}", dtype=torch.bfloat16)
+        out = {"case": case, "gflop": 2.0 * N * H * W * C * 9 * C / 1e9}
+        for path, name in ((0, "tcgen05"), (1, "mma_sync")):
+            K.set_conv_path(path)
+            for _ in range(3):
+                K.conv3x3(x, N, H, W, C, C, w, None, y, C, C, True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(20):
+                K.conv3x3(x, N, H, W, C, C, w, None, y, C, C, True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 20
+            out[name] = {"ms": ms, "tflops": out["gflop"] / ms}
+        K.set_conv_path(0)
+        print(json.dumps(out))
+    else:
+        raise SystemExit(f"unknown case {case}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -526,7 +592,12 @@ def main():
                     help="skip the 64-frame movie and the 1024x1024 / 2e6-visibility image")
     ap.add_argument("--warm-problems", type=int, default=256,
                     help="held-out problems of the learned warm-start comparison (0: skip)")
+    ap.add_argument("--case", default=None, choices=["traffic", "fg", "t2", "t1", "conv"],
+                    help="run one small launch for a profiler capture instead of the benchmark")
     args = ap.parse_args()
+    if args.case:
+        profile_case(args.case)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
