@@ -31,7 +31,10 @@ int smili_unet_conv3x3(const void* x, int N, int H, int W, int Cin, int ldx, con
 
 /* dw (+)= sum over pixels of dy[p][co] x[p + (ky-1, kx-1)][ci].  `partial` is
  * scratch of nsplit * Cout * 9 * Cin floats; the splits are summed in a fixed
- * order, so the result is deterministic. */
+ * order, so the result is deterministic.  When Cin, Cout, ldx and lddy are
+ * multiples of 8 and x, dy are 16-byte aligned, the partials come from the
+ * tcgen05 tensor cores (pixels as the K dimension, both operands TMA-staged);
+ * otherwise from mma.sync. */
 int smili_unet_conv3x3_wgrad(const void* x, int ldx, const void* dy, int lddy, int N, int H, int W, int Cin,
                              int Cout, float* partial, int nsplit, float* dw, int accumulate, void* stream);
 
@@ -67,14 +70,15 @@ int smili_unet_adam(float* w, void* w16, const float* g, float* m, float* v, lon
 
 int smili_unet_f32_to_bf16(const float* x, void* y, long long n, void* stream);
 
-/* Convolution path: 0 (default) tcgen05 where it applies, 1 mma.sync always.
- * Process-wide; for comparisons and tests. */
+/* Convolution path (forward, data gradient and weight gradient): 0 (default)
+ * tcgen05 where it applies, 1 mma.sync always.  Process-wide; for comparisons
+ * and tests. */
 int smili_unet_set_conv_path(int path);
 
 /* Reads and clears the tcgen05 convolution's error flag (synchronous):
  * 0, or the code of a bounded wait inside the kernel that ran out (1 stage
- * release, 2 operand arrival, 3 accumulator completion, 4 outstanding copy),
- * or SMILI_UNET_ERR_CUDA. */
+ * release, 2 operand arrival, 3 accumulator completion, 4 outstanding copy;
+ * 5-8 the same in the weight gradient), or SMILI_UNET_ERR_CUDA. */
 int smili_unet_tc_status(void);
 
 /* Why the last tcgen05 convolution call of this thread failed ("" if none). */

@@ -293,6 +293,176 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
 }
 
 // ---------------------------------------------------------------------------
+// conv3x3 weight gradient on tcgen05:
+//   dW[co][tap][ci] = sum over pixels p of dY[p][co] X[p + s(tap)][ci]
+// One CTA per (split, tap, M tile, N tile); the K dimension is pixels, one
+// 8 x 16 pixel tile (128 K rows) per stage, eight UMMA K-steps of 16.  Both
+// operands are MN-major: a TMA box of 64 channels x 16 x 8 pixels of the NHWC
+// tensor is 128 rows (pixels, the K index) of 128 bytes (64 channels of the
+// M or N index) in the 128-byte swizzle, the canonical MN-major SWIZZLE_128B
+// layout (8-row atoms 1024 bytes apart along K: the stride byte offset; the
+// next 64 channels in the next box, 16 KB on: the leading byte offset).
+// The larger of (Cout, Cin) is the M side (128, padded by TMA zero fill),
+// the smaller the N side (a multiple of 16 up to 256): with 24 channels an
+// N of 32 wastes far less than an M of 128.  X is read at the tap-shifted
+// coordinates (zeros outside the image), dY unshifted.  Each split writes
+// its own FP32 partial [split][co][tap][ci]; the splits are summed later in
+// a fixed order, so the result is deterministic.
+// ---------------------------------------------------------------------------
+constexpr int WG_BOX = 64;                       // channels per TMA box (128 bytes)
+constexpr uint32_t WG_BOX_BYTES = 128 * 128;     // 128 pixels x 128 bytes
+
+struct WgParams {
+  int H, W, Cin, Cout;
+  int tiles_x, tiles_y, ntiles, nsplit;
+  int m_is_ci;            // 0: M = output channels (A = dY); 1: M = input channels (A = X)
+  int mtiles, ntile, nboxes_n, ntiles_n;
+  int tmem_cols, stages;
+  float* partial;
+};
+
+__device__ __forceinline__ uint64_t sdesc_mn_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(WG_BOX_BYTES >> 4) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// kind::f16 instruction descriptor: D f32, A and B bf16, both MN-major
+__host__ __device__ constexpr uint32_t idesc_bf16_mn(int ntile) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(ntile >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(128) conv3x3_wgrad_tc_kernel(const __grid_constant__ CUtensorMap tmdy,
+                                                               const __grid_constant__ CUtensorMap tmx,
+                                                               WgParams p) {
+  extern __shared__ unsigned char dyn_raw[];
+  __shared__ __align__(8) uint64_t full_bar[4], empty_bar[4], done_bar;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int consumed;
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~uintptr_t(1023));
+  const int S = p.stages;
+  const uint32_t stage_bytes = (uint32_t)(2 + p.nboxes_n) * WG_BOX_BYTES;  // A: 2 boxes (M = 128)
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int split = blockIdx.x;
+  int rest = blockIdx.y;
+  const int tap = rest % 9;
+  rest /= 9;
+  const int mt = rest % p.mtiles;
+  const int nt = rest / p.mtiles;
+  const int ky = tap / 3, kx = tap - ky * 3;
+  const int m0 = mt * 128, n0 = nt * p.ntile;
+  int nk = 0;  // pixel tiles of this split
+  if (split < p.ntiles) nk = (p.ntiles - 1 - split) / p.nsplit + 1;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&done_bar, 1);
+    consumed = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"((uint32_t)p.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  int issued = 0;
+  if (warp == 0 && lane == 0) {
+    for (int k = 0; k < nk; ++k) {
+      const int s = k % S;
+      if (k >= S && !mbar_wait(&empty_bar[s], ((k / S) - 1) & 1)) {
+        set_err(5);
+        break;
+      }
+      const int t = split + k * p.nsplit;
+      const int tx = t % p.tiles_x, ty = (t / p.tiles_x) % p.tiles_y, n = t / (p.tiles_x * p.tiles_y);
+      const int x0 = tx * TILE_W, y0 = ty * TILE_H;
+      unsigned char* st = base + (size_t)s * stage_bytes;
+      mbar_expect_tx(&full_bar[s], stage_bytes);
+      // A (M side, 2 boxes of 64 channels) then B (N side)
+      for (int b = 0; b < 2 + p.nboxes_n; ++b) {
+        const bool is_a = b < 2;
+        const int c0 = is_a ? m0 + b * WG_BOX : n0 + (b - 2) * WG_BOX;
+        const bool use_x = is_a == (p.m_is_ci != 0);  // which tensor this box comes from
+        if (use_x)
+          tma_load_4d(st + b * WG_BOX_BYTES, &tmx, &full_bar[s], c0, x0 + kx - 1, y0 + ky - 1, n);
+        else
+          tma_load_4d(st + b * WG_BOX_BYTES, &tmdy, &full_bar[s], c0, x0, y0, n);
+      }
+      issued = k + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    const uint32_t idesc = idesc_bf16_mn(p.ntile);
+    int k = 0;
+    for (; k < nk; ++k) {
+      const int s = k % S;
+      if (!mbar_wait(&full_bar[s], (k / S) & 1)) {
+        set_err(6);
+        break;
+      }
+      fence_after();
+      const uint32_t a = smem_u32(base + (size_t)s * stage_bytes);
+      const uint32_t b = a + 2 * WG_BOX_BYTES;
+#pragma unroll
+      for (int ks = 0; ks < 8; ++ks)  // 16 pixels (K rows) of 128 bytes per step
+        umma_bf16(tmem, sdesc_mn_sw128(a + ks * 2048), sdesc_mn_sw128(b + ks * 2048), idesc,
+                  (k > 0 || ks > 0) ? 1u : 0u);
+      umma_commit(&empty_bar[s]);
+    }
+    consumed = k;
+    umma_commit(&done_bar);
+  }
+  __syncwarp();
+  if (!mbar_wait(&done_bar, 0)) set_err(7);
+  fence_after();
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    for (int k = consumed; k < issued; ++k)
+      if (!mbar_wait(&full_bar[k % S], (k / S) & 1)) set_err(8);
+  }
+
+  // epilogue: accumulator row (M index) 32w + lane, columns the N index
+  const int mrow = m0 + warp * 32 + lane;
+  const int mlim = p.m_is_ci ? p.Cin : p.Cout, nlim = p.m_is_ci ? p.Cout : p.Cin;
+  float* part = p.partial + (size_t)split * p.Cout * 9 * p.Cin;
+  for (int c = 0; c < p.ntile; c += 16) {
+    float v[16];
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    if (mrow >= mlim || nk == 0) {
+      if (nk == 0 && mrow < mlim) {  // a split without pixels still writes its (zero) partial
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = 0.f;
+      } else {
+        continue;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int ncol = n0 + c + i;
+      if (ncol >= nlim) break;
+      const int co = p.m_is_ci ? ncol : mrow, ci = p.m_is_ci ? mrow : ncol;
+      part[((size_t)co * 9 + tap) * p.Cin + ci] = v[i];
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 2) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)p.tmem_cols)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -398,6 +568,79 @@ inline int launch(const __nv_bfloat16* x, int N, int H, int W, int Cin, int ldx,
   cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   conv3x3_tc_kernel<<<dim3((unsigned)tiles, (Cout + ntile - 1) / ntile), 128, smem, stream>>>(mx, mw, p);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(std::string("launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+// Whether the tensor-core weight gradient applies: TMA needs 16-byte row
+// strides and bases (channel strides multiples of 8).
+inline bool wgrad_eligible(const void* x, int ldx, const void* dy, int lddy, int Cin, int Cout) {
+  return ldx % 8 == 0 && lddy % 8 == 0 && Cin % 8 == 0 && Cout % 8 == 0 &&
+         (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (reinterpret_cast<uintptr_t>(dy) & 15) == 0 &&
+         encode_fn() != nullptr;
+}
+
+inline int encode_act(CUtensorMap* m, const __nv_bfloat16* t, int C, int ld, int W, int H, int N) {
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+  const cuuint64_t strides[3] = {(cuuint64_t)ld * 2, (cuuint64_t)W * ld * 2, (cuuint64_t)H * W * ld * 2};
+  const cuuint32_t box[4] = {WG_BOX, TILE_W, TILE_H, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(t), dims,
+                                 strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
+// partial[nsplit][Cout][9][Cin] (FP32); returns 0 or a negative code
+inline int launch_wgrad(const __nv_bfloat16* x, int ldx, const __nv_bfloat16* dy, int lddy, int N, int H, int W,
+                        int Cin, int Cout, float* partial, int nsplit, cudaStream_t stream) {
+  last_error().clear();
+  if (!encode_fn()) return fail("cuTensorMapEncodeTiled is not available from the driver");
+  WgParams p;
+  p.H = H;
+  p.W = W;
+  p.Cin = Cin;
+  p.Cout = Cout;
+  p.tiles_x = (W + TILE_W - 1) / TILE_W;
+  p.tiles_y = (H + TILE_H - 1) / TILE_H;
+  const long long ntiles = (long long)p.tiles_x * p.tiles_y * N;
+  if (ntiles > 0x7fffffffLL) {
+    last_error() = "too many pixel tiles";
+    return -1;
+  }
+  p.ntiles = (int)ntiles;
+  p.nsplit = nsplit;
+  p.m_is_ci = Cin > Cout;
+  const int mdim = p.m_is_ci ? Cin : Cout, ndim = p.m_is_ci ? Cout : Cin;
+  p.mtiles = (mdim + 127) / 128;
+  p.ntiles_n = (ndim + 255) / 256;
+  const int nper = (ndim + p.ntiles_n - 1) / p.ntiles_n;
+  p.ntile = (nper + 15) / 16 * 16;
+  p.nboxes_n = (p.ntile + WG_BOX - 1) / WG_BOX;
+  int cols = 32;
+  while (cols < p.ntile) cols *= 2;
+  p.tmem_cols = cols;
+  const size_t stage = (size_t)(2 + p.nboxes_n) * WG_BOX_BYTES;
+  p.stages = (int)std::max<size_t>(2, std::min<size_t>(4, (200 * 1024 - 1024) / stage));
+  size_t smem = 1024 + stage * p.stages;
+  const size_t min_for_tmem = (size_t)228 * 1024 / (512 / cols + 1) + 1024;
+  if (smem < min_for_tmem) smem = min_for_tmem;
+  if (smem > 227 * 1024) {
+    last_error() = "shared memory of the weight-gradient stages too large";
+    return -1;
+  }
+  p.partial = partial;
+  CUtensorMap mdy, mx;
+  int r = encode_act(&mdy, dy, Cout, lddy, W, H, N);
+  if (r) return fail("tensor map of the output gradient: CUresult " + std::to_string(r));
+  r = encode_act(&mx, x, Cin, ldx, W, H, N);
+  if (r) return fail("tensor map of the input: CUresult " + std::to_string(r));
+  cudaError_t e =
+      cudaFuncSetAttribute(conv3x3_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return fail(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  const long long gy = 9LL * p.mtiles * p.ntiles_n;
+  conv3x3_wgrad_tc_kernel<<<dim3((unsigned)nsplit, (unsigned)gy), 128, smem, stream>>>(mdy, mx, p);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(std::string("launch: ") + cudaGetErrorString(e));
   return 0;

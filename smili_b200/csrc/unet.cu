@@ -17,8 +17,10 @@
 // implicit GEMM over pixels with deterministic per-split partial sums.
 // Convolutions whose input rows and weights TMA can address (Cin and the
 // channel stride multiples of 8, 16-byte aligned bases) run instead on the
-// tcgen05 tensor cores with the accumulator in tensor memory (conv_tc.cuh);
-// the mma.sync kernel below takes the rest (the one-channel input layer).
+// tcgen05 tensor cores with the accumulator in tensor memory (conv_tc.cuh),
+// and so do weight gradients whose channel counts and strides are multiples
+// of 8; the mma.sync kernels below take the rest (the one-channel input and
+// output layers).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -494,7 +496,12 @@ int smili_unet_conv3x3_wgrad(const void* x, int ldx, const void* dy, int lddy, i
   a.nsplit = nsplit;
   a.partial = partial;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  conv3x3_wgrad_kernel<<<dim3(nsplit, (Cout + 63) / 64, (Cin + KC - 1) / KC), 256, 0, s>>>(a);
+  if (g_conv_path != 1 && tc::wgrad_eligible(x, ldx, dy, lddy, Cin, Cout)) {
+    if (tc::launch_wgrad(a.x, ldx, a.dy, lddy, N, H, W, Cin, Cout, partial, nsplit, s) != 0)
+      return SMILI_UNET_ERR_CUDA;
+  } else {
+    conv3x3_wgrad_kernel<<<dim3(nsplit, (Cout + 63) / 64, (Cin + KC - 1) / KC), 256, 0, s>>>(a);
+  }
   const size_t count = (size_t)Cout * 9 * Cin;
   sum_partials_kernel<<<grid_for(count), 256, 0, s>>>(partial, nsplit, count, dw, accumulate);
   return check_launch();

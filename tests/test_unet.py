@@ -156,7 +156,8 @@ def test_conv3x3_tcgen05_matches_mma_sync(N, H, W, Cin, Cout):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("N,H,W,Cin,Cout", [(2, 16, 16, 1, 24), (2, 32, 32, 24, 24), (1, 16, 16, 288, 96),
-                                            (2, 8, 8, 96, 192), (1, 12, 20, 20, 1)])
+                                            (2, 8, 8, 96, 192), (1, 12, 20, 20, 1), (3, 24, 40, 144, 48),
+                                            (2, 16, 16, 72, 24), (1, 8, 16, 48, 96)])
 def test_conv3x3_wgrad_kernel(N, H, W, Cin, Cout):
     import torch
     from smili_b200.warmstart import kernels as K
@@ -166,10 +167,16 @@ def test_conv3x3_wgrad_kernel(N, H, W, Cin, Cout):
     nsplit = 7
     partial = torch.zeros(nsplit * Cout * 9 * Cin, dtype=torch.float32, device="cuda")
     dw = torch.zeros(Cout * 9 * Cin, dtype=torch.float32, device="cuda")
-    K.conv3x3_wgrad(_bf16_tensor(x), Cin, _bf16_tensor(dy), Cout, N, H, W, Cin, Cout, partial, nsplit, dw)
     want = U.conv3x3_wgrad(x, dy)
-    got = dw.cpu().numpy().reshape(want.shape)
-    assert np.max(np.abs(got - want)) <= 1e-4 * np.max(np.abs(want))
+    try:
+        for path in (0, 1):  # tcgen05 (where the channel counts allow), then mma.sync
+            K.set_conv_path(path)
+            K.conv3x3_wgrad(_bf16_tensor(x), Cin, _bf16_tensor(dy), Cout, N, H, W, Cin, Cout, partial, nsplit, dw)
+            got = dw.cpu().numpy().reshape(want.shape)
+            assert np.max(np.abs(got - want)) <= 1e-4 * np.max(np.abs(want)), path
+    finally:
+        K.set_conv_path(0)
+    assert K.tc_status() == 0
     db = torch.zeros(Cout, dtype=torch.float32, device="cuda")
     K.bias_grad(_bf16_tensor(dy), Cout, N * H * W, Cout, db)
     np.testing.assert_allclose(db.cpu().numpy(), dy.reshape(-1, Cout).sum(0), rtol=1e-4, atol=1e-3)
