@@ -21,15 +21,20 @@ four times per seed, in one batch).  ``value`` counts only the solves that
 reached their plain solve's final cost (x (1 + target_rtol)) within its
 iteration budget; ``value_all`` counts every solve of the launch.
 
-One step = one batched FP32 solve of ``--batch`` problems (device-resident
-inputs, one persistent launch).  The batch holds more problems than
-resident CTA groups: a group whose problem reaches its target takes the next
-queued problem, so early exits shorten the launch.  The group size is chosen
-by ``smili_b200.autotune`` from whole solves of this batch with its targets.
+One step = one batched FP32 solve of ``--batch`` problems with inputs
+resident on the device.  The batch holds more problems than resident CTA
+groups: a group whose problem reaches its target takes the next queued
+problem, so early exits shorten the launch.  The group size is chosen by
+``smili_b200.autotune`` from whole solves of this batch with its targets.
+With the trained weights present the step is the learned warm start
+(``WarmStart``): 50 FP32 iterations from the prior, the U-Net's proposal
+from those images, and the remaining iterations from the proposals; the
+cold arm (every problem from its prior) is timed beside it (``value_cold``).
 ``value`` = counted solves per second over the timed steps; ``e2e`` = the
-same metric through the C ABI from host buffers (upload, solve, download of
-every image inside the timed region); ``plain_fp64`` reports single-problem
-FP64 solves/s; ``cpu_baseline`` times the CPU restatement (one whole solve).
+same metric through the C ABI from host buffers (packing and upload of the
+problems, the step, download of every image inside the timed region);
+``plain_fp64`` reports single-problem FP64 solves/s; ``cpu_baseline`` times
+the CPU restatement (one whole solve).
 ``--impl reference`` times only that CPU path (the reference's
 Fortran/FINUFFT build is unavailable in this image).
 
@@ -52,12 +57,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # DRAM bytes per function/gradient evaluation of the FP32 batched solver on
-# this workload: one ncu capture of a 74-problem launch (2 CTAs of 512
-# threads per problem) measured dram__bytes_read.sum + dram__bytes_write.sum
-# = 96.23 GB over 1197 evaluations.  The per-evaluation traffic does not
-# depend on the batch size, so a launch's traffic scales with its evaluation
-# count.
-DRAM_BYTES_PER_EVAL_FP32 = 96.23e9 / 1197
+# this workload at the benchmark's concurrency (74 resident groups of 4
+# CTAs of 512 threads): one ncu capture of ``bench.py --case traffic`` (74
+# problems, 20 iterations) measured dram__bytes_read.sum +
+# dram__bytes_write.sum = 186.83 + 40.00 GB over 2261 evaluations.  The
+# traffic of a step scales with its evaluation count.
+DRAM_BYTES_PER_EVAL_FP32 = (186.83e9 + 40.00e9) / 2261
 
 METRIC = "imaging solves/s at 256²/1e5 vis, FP32+batched+warm-start vs plain, equal final χ²"
 WORKLOAD = ("256x256 / 97 200 uv points (amp 5% + cp + lca), l1/TV/MEM = 1/1/0.1, L-BFGS-B m=5, "
@@ -272,57 +277,81 @@ def warm_start_cfg4(nprob, niter, rtol, device=0, group=4):
             "nrmse_truth_warm_fp32": nr(xs_w)}
 
 
-def warm_start_headline(probs, kws, seed_of, ftarget, niter, G, cold_ms, cold_hits, device=0):
-    """The learned warm start on this workload (``smili_b200.warmstart.closure``):
-    K FP32 iterations from the prior, the U-Net's proposal from that image,
-    then FP32 L-BFGS-B with the remaining budget, all problems batched as in
-    the cold arm with the same targets.  Its time is the two launches' device
-    time plus the proposal (network forward pass on the device and the host
-    work that turns images into starting vectors).  Reported beside the cold
-    arm's solves/s; problems that reach their target in the first K
-    iterations count as solved there."""
-    import torch
-    from smili_b200 import _lib
-    from smili_b200.warmstart import closure, data
-    from smili_b200.warmstart.unet import UNet
-    path = os.path.join(ROOT, "smili_b200", "warmstart", "unet_closure256.npz")
-    if not os.path.exists(path):
-        return {"unavailable": "trained weights smili_b200/warmstart/unet_closure256.npz missing"}
-    net = UNet.load(path, device=f"cuda:{device}")
-    K = closure.K_DEFAULT
-    B = len(probs)
-    opts = _lib.make_options(32, 1e-6, G, device)
-    bk = _lib.Batch(probs, niter=K, options=opts)
-    bk.set_targets(ftarget)
-    ms_k = bk.run()
-    early = [bk.fetch(p) for p in range(B)]
-    bk.close()
-    t0 = time.perf_counter()
-    imgs = closure.normalise([data.to_grid(kws[seed_of[p]], early[p][0]) for p in range(B)])
-    t_host = time.perf_counter() - t0
-    net.predict(imgs[:8])  # first-call set-up outside the timing
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    pred = net.predict(imgs)
-    e1.record()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    x0 = [closure.warm_init(kws[seed_of[p]], pred[p], early[p][0]) for p in range(B)]
-    wprobs = [_lib.Problem(dict(kws[seed_of[p]], iin=x0[p])) for p in range(B)]
-    t_host += time.perf_counter() - t0
-    bw = _lib.Batch(wprobs, niter=niter - K, options=opts)
-    bw.set_targets(ftarget)
-    ms_w = bw.run()
-    hit_k = np.array([e[3]["task"] == _lib.TASK_TARGET for e in early])
-    hit_w = np.array([bw.fetch(p)[3]["task"] == _lib.TASK_TARGET for p in range(B)])
-    bw.close()
-    hits = int((hit_k | hit_w).sum())
-    t = ms_k / 1000.0 + e0.elapsed_time(e1) / 1000.0 + t_host + ms_w / 1000.0
-    return {"K": K, "problems": B, "reached_target": hits, "solves_per_s": hits / t,
-            "cold_solves_per_s": cold_hits / (cold_ms / 1000.0),
-            "parts_s": {"first_K_iterations_device": ms_k / 1000.0,
-                        "unet_forward_device": e0.elapsed_time(e1) / 1000.0, "host": t_host,
-                        "warm_solve_device": ms_w / 1000.0}}
+UNET_FORWARD_LAUNCHES = 21  # 15 convolutions, 3 poolings, 3 upsamplings per forward pass
+
+
+class WarmStart:
+    """The learned warm start on this workload (``smili_b200.warmstart.closure``).
+
+    One step: K FP32 iterations of every problem from its prior (one
+    launch), the U-Net's proposal from each K-iteration image, then the
+    remaining niter - K FP32 iterations from the proposals (a second launch
+    of the same device-resident problems, restarted with
+    ``Batch.set_start``), with the same targets as the cold arm.  A problem
+    that reaches its target in the first K iterations counts there and
+    restarts from its own image.  The step's time is the two launches' CUDA
+    event times, the network's forward pass (CUDA events) and the host work
+    between them (fetching the K-iteration images, forming the network
+    input, turning its output into starting vectors and uploading them;
+    wall clock)."""
+
+    def __init__(self, probs, kws, seed_of, ftarget, niter, G, device=0):
+        import torch
+        from smili_b200 import _lib
+        from smili_b200.warmstart import closure
+        from smili_b200.warmstart.unet import UNet
+        self.torch, self.lib, self.closure = torch, _lib, closure
+        self.net = UNet.load(WARM_WEIGHTS, device=f"cuda:{device}")
+        self.K = closure.K_DEFAULT
+        self.kws, self.seed_of, self.B = kws, seed_of, len(probs)
+        self.opts = _lib.make_options(32, 1e-6, G, device)
+        self.bk = _lib.Batch(probs, niter=self.K, options=self.opts)
+        self.bk.set_targets(ftarget)
+        self.bw = _lib.Batch(probs, niter=niter - self.K, options=self.opts)
+        self.bw.set_targets(ftarget)
+        nx = int(kws[0]["nx"])
+        self.net.predict(np.zeros((self.B, nx, nx), np.float32), batch=self.B)  # buffers and first-call set-up
+
+    def step(self):
+        from smili_b200.warmstart import data
+        torch, _lib, closure, B = self.torch, self.lib, self.closure, self.B
+        ms_k = self.bk.run()
+        t0 = time.perf_counter()
+        early = [self.bk.fetch(p) for p in range(B)]
+        imgs = closure.normalise([data.to_grid(self.kws[self.seed_of[p]], early[p][0]) for p in range(B)])
+        t_host = time.perf_counter() - t0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        pred = self.net.predict(imgs, batch=B)
+        e1.record()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hit_k = np.array([e[3]["task"] == _lib.TASK_TARGET for e in early])
+        for p in range(B):
+            x0 = early[p][0] if hit_k[p] else closure.warm_init(self.kws[self.seed_of[p]], pred[p], early[p][0])
+            self.bw.set_start(p, x0)
+        t_host += time.perf_counter() - t0
+        ms_w = self.bw.run()
+        infos = [self.bw.fetch(p)[3] for p in range(B)]
+        hit = hit_k | np.array([i["task"] == _lib.TASK_TARGET for i in infos])
+        ms_net = e0.elapsed_time(e1)
+        return {"s": (ms_k + ms_net + ms_w) / 1000.0 + t_host, "hits": int(hit.sum()),
+                "kernel_s": (ms_k + ms_w) / 1000.0,
+                "nfg": int(sum(e[3]["nfg"] for e in early) + sum(i["nfg"] for i in infos)),
+                "iterations": int(sum(self.K if h else self.K + i["niter"] for h, i in zip(hit_k, infos))),
+                "parts_s": {"first_K_iterations_device": ms_k / 1000.0, "unet_forward_device": ms_net / 1000.0,
+                            "host": t_host, "remaining_iterations_device": ms_w / 1000.0}}
+
+    def fetch(self, p):
+        return self.bw.fetch(p)
+
+    def close(self):
+        self.bk.close()
+        self.bw.close()
+
+
+WARM_WEIGHTS = os.path.join(ROOT, "smili_b200", "warmstart", "unet_closure256.npz")
+WARM_K = 50  # FP32 iterations before the proposal (smili_b200.warmstart.closure.K_DEFAULT)
 
 
 def survey_cfg3(nprob, niter, device=0, nplain=8):
@@ -590,6 +619,8 @@ def main():
                     help="problems of the batched survey configuration (0: skip)")
     ap.add_argument("--no-config5", dest="config5", action="store_false",
                     help="skip the 64-frame movie and the 1024x1024 / 2e6-visibility image")
+    ap.add_argument("--no-warm", action="store_true",
+                    help="time the cold arm (prior starts) as the headline instead of the learned warm start")
     ap.add_argument("--warm-problems", type=int, default=256,
                     help="held-out problems of the learned warm-start comparison (0: skip)")
     ap.add_argument("--case", default=None, choices=["traffic", "fg", "t2", "t1", "conv"],
@@ -686,50 +717,91 @@ def main():
         tuned = autotune.tune(probs, 32, niter=args.niter, repeats=1, device=local,
                               cands=[(3, 8), (4, 8)], targets=targets[seed_of])
     # FP32 batched, inputs resident on the device: the reference's iteration
-    # budget with an early exit at the plain solve's final cost
+    # budget with an early exit at the plain solve's final cost.  The cold
+    # arm starts every problem from its prior; the warm arm (the headline
+    # when the trained weights are present) from the U-Net's proposal.
     opts = _lib.make_options(32, 1e-6, tuned["ctas_per_problem"], local, spread_bin=tuned["spread_bin"])
     ftarget = targets[seed_of]
+    warm = (not args.no_warm) and os.path.exists(WARM_WEIGHTS)
     batch = _lib.Batch(probs, niter=args.niter, options=opts)
     batch.set_targets(ftarget)
-    for _ in range(args.warmup):
+    cold_warmup, cold_steps = (1, 2) if warm else (args.warmup, args.steps)
+    for _ in range(cold_warmup):
         batch.run()
-    if dist:
+    if dist and not warm:
         dist.barrier()
-    times, step_hits = [], []
+    cold_times, cold_hits = [], []
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            times.append(batch.run())
-            step_hits.append(hits(batch, B))  # between timed launches, outside the events
-    ms_step = float(np.mean(times))
-    fp32 = quality(batch, B, seed_of)
-    nfg = sum(batch.fetch(p)[3]["nfg"] for p in range(B))
-    fp32["nfg_total"] = int(nfg)
-    iters = int(sum(batch.fetch(p)[3]["niter"] for p in range(B)))
-    fp32["reached_target_per_step"] = step_hits
-    reached = float(np.mean(step_hits))
-    # stage profile of one extra (untimed) step
+        for _ in range(cold_steps):
+            cold_times.append(batch.run())
+            cold_hits.append(hits(batch, B))  # between timed launches, outside the events
+    cold = quality(batch, B, seed_of)
+    cold_nfg = sum(batch.fetch(p)[3]["nfg"] for p in range(B))
+    cold_iters = int(sum(batch.fetch(p)[3]["niter"] for p in range(B)))
+    cold["nfg_total"] = int(cold_nfg)
+    cold["reached_target_per_step"] = cold_hits
+    cold["ms_per_step"] = float(np.mean(cold_times))
+    cold["value"] = world * float(np.mean(cold_hits)) / (cold["ms_per_step"] / 1000.0)
+    # stage profile of one extra (untimed) cold step
     batch.profile(True)
     batch.run()
     stages = batch.stage_times()
     batch.profile(False)
     batch.close()
 
+    h2d_prob = sum(arr.nbytes for p in probs for arr in p.keep.values())
+    npix_all = sum(p.npix for p in probs)
+    if warm:
+        ws = WarmStart(probs, kws, seed_of, ftarget, args.niter, tuned["ctas_per_problem"], local)
+        for _ in range(args.warmup):
+            ws.step()
+        if dist:
+            dist.barrier()
+        steps = []
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                steps.append(ws.step())
+        ms_step = 1000.0 * float(np.mean([r["s"] for r in steps]))
+        kernel_s = float(np.mean([r["kernel_s"] for r in steps]))
+        step_hits = [r["hits"] for r in steps]
+        fp32 = quality(ws, B, seed_of)
+        nfg, iters = steps[-1]["nfg"], steps[-1]["iterations"]
+        fp32["nfg_total"] = int(nfg)
+        fp32["reached_target_per_step"] = step_hits
+        fp32["parts_s"] = {k: float(np.mean([r["parts_s"][k] for r in steps])) for k in steps[0]["parts_s"]}
+        ws.close()
+        launches = UNET_FORWARD_LAUNCHES + 2
+        # end to end from host buffers: packing and upload of both launches'
+        # problems, the step (its start images uploaded inside), download
+        h2d = 2 * h2d_prob + 8 * npix_all
+        d2h = 2 * (2 * 8 * npix_all + 15 * 8 * B) + 8 * npix_all
+    else:
+        ms_step, kernel_s = cold["ms_per_step"], cold["ms_per_step"] / 1000.0
+        step_hits, fp32 = cold_hits, cold
+        nfg, iters = cold_nfg, cold_iters
+        launches = 1
+        h2d, d2h = h2d_prob, sum(8 * p.npix + 15 * 8 for p in probs)
+    reached = float(np.mean(step_hits))
+
     # end to end through the C ABI from host buffers
     e2e_times, e2e_hits = [], []
-    h2d = 0
-    for p in probs:
-        for arr in p.keep.values():
-            h2d += arr.nbytes
-    d2h = sum(8 * p.npix + 15 * 8 for p in probs)
     for _ in range(max(0, args.e2e_steps)):
         t0 = time.perf_counter()
-        b2 = _lib.Batch(probs, niter=args.niter, options=opts)
-        b2.set_targets(ftarget)
-        b2.run()
-        got = [b2.fetch(p) for p in range(B)]
-        b2.close()
+        if warm:
+            w2 = WarmStart(probs, kws, seed_of, ftarget, args.niter, tuned["ctas_per_problem"], local)
+            r = w2.step()
+            for p in range(B):
+                w2.fetch(p)
+            w2.close()
+            e2e_hits.append(r["hits"])
+        else:
+            b2 = _lib.Batch(probs, niter=args.niter, options=opts)
+            b2.set_targets(ftarget)
+            b2.run()
+            got = [b2.fetch(p) for p in range(B)]
+            b2.close()
+            e2e_hits.append(int(sum(g[3]["task"] == _lib.TASK_TARGET for g in got)))
         e2e_times.append(time.perf_counter() - t0)
-        e2e_hits.append(int(sum(g[3]["task"] == _lib.TASK_TARGET for g in got)))
 
     e2e_mean = float(np.mean(e2e_times)) if e2e_times else float("nan")
     max_ms, e2e_s = max_over_ranks(dist, ms_step, e2e_mean, "cuda")
@@ -739,7 +811,7 @@ def main():
     value_all, value, _ = job_values(world, B, reached, max_ms, e2e_s)
     e2e_value = world * float(np.mean(e2e_hits)) / e2e_s if e2e_hits else float("nan")
     bfg = fg_bytes(kws[0], 4)
-    achieved = bfg * nfg / (ms_step / 1000.0) / 1e9
+    achieved = bfg * nfg / kernel_s / 1e9
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -762,11 +834,15 @@ def main():
                                                 "autotuner (whole solves of this batch with its targets)"),
                                   "autotune_ms": [r["ms"] for r in tuned.get("table", [])]},
                        "precision": "FP32 transforms + compensated chi-square, FP64 L-BFGS-B",
-                       "warm_start": "none in value (cold starts from the prior); the learned warm "
-                                     "start is measured in warm_start_cfg4",
+                       "warm_start": ("learned (smili_b200/warmstart/unet_closure256.npz): the U-Net's "
+                                      f"proposal from the image after {WARM_K} FP32 iterations starts the "
+                                      "remaining iterations; its time is inside value" if warm else
+                                      "none (cold starts from the prior)"),
                        "l2": "inputs larger than L2 (batch footprint >> 126 MB)",
                        "parallelism": f"replicas x{world}"},
             "value_all": value_all,
+            "value_cold": cold["value"],
+            "quality_fp32_cold": cold,
             "plain_fp64": {"value": 1000.0 * S / float(np.sum(plain_ms)), "unit": "solves/s",
                            "ms_per_solve": float(np.mean(plain_ms)),
                            "nfg_mean": float(np.mean(plain_nfg)),
@@ -780,14 +856,15 @@ def main():
                          "traffic": DRAM_BYTES_PER_EVAL_FP32 * nfg / 1e9,
                          "traffic_unit": "GB per launch (ncu, scaled by evaluations)",
                          "kernel": "smili_batch_kernel<float> (persistent solve)",
-                         "algorithmic_bytes_per_eval": bfg, "evals_per_launch": nfg,
+                         "algorithmic_bytes_per_eval": bfg, "evals_per_step": nfg,
+                         "kernel_s_per_step": kernel_s,
                          "peak_source": "measured" if peaks else "fallback"},
             "roofline_with_optimizer": {
                 "bound": "hbm", "unit": "GB/s", "peak": peak,
-                "achieved": (bfg * nfg + lb_bytes_per_iteration(kws[0]) * iters) / (ms_step / 1000.0) / 1e9,
-                "frac": (bfg * nfg + lb_bytes_per_iteration(kws[0]) * iters) / (ms_step / 1000.0) / 1e9 / peak,
+                "achieved": (bfg * nfg + lb_bytes_per_iteration(kws[0]) * iters) / kernel_s / 1e9,
+                "frac": (bfg * nfg + lb_bytes_per_iteration(kws[0]) * iters) / kernel_s / 1e9 / peak,
                 "bytes_per_iteration_lbfgsb": lb_bytes_per_iteration(kws[0]), "iterations_per_launch": iters},
-            "gpu_launches": args.steps,
+            "gpu_launches": launches * args.steps,
             "clocks": clk.summary(),
             "stage_ms_problem0": {k: round(v, 3) for k, v in stages.items()},
         }
@@ -796,8 +873,6 @@ def main():
             line["large_cfg5"] = large_cfg5(args.niter, local)
         if args.survey > 0:
             line["survey_cfg3"] = survey_cfg3(args.survey, args.niter, local)
-        line["warm_start_headline"] = warm_start_headline(
-            probs, kws, seed_of, ftarget, args.niter, tuned["ctas_per_problem"], ms_step, reached, local)
         if args.warm_problems > 0:
             line["warm_start_cfg4"] = warm_start_cfg4(args.warm_problems, args.niter, args.target_rtol, local)
         if not args.no_cpu:

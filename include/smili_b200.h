@@ -121,6 +121,13 @@ int smili_batch_fetch(smili_batch* b, int p, double* iout, double* terms, double
  * with SMILI_TASK_TARGET at the first completed iteration whose cost is
  * <= ftarget[p]; niter stays the iteration cap.  NULL clears the targets. */
 int smili_batch_set_targets(smili_batch* b, const double* ftarget);
+
+/* Replace problem p's start image (no reference counterpart): the npix
+ * pixel values x (in the kwargs' scaled units) become the initial image of
+ * the next smili_batch_run, as `iin` at packing did.  Lets a caller restart
+ * a device-resident batch from new images (a warm start) without packing
+ * and uploading its data again.  Movies are not supported. */
+int smili_batch_set_start(smili_batch* b, int p, const double* x);
 /* Cost recorded at each completed iteration of problem p (NaN where absent). */
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len);
 void smili_batch_destroy(smili_batch* b);

@@ -105,7 +105,7 @@ EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "sm
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
            "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile",
            "smili_batch_set_targets", "smili_calc_cost_noalloc", "smili_fftim3d_imaging",
-           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist"]
+           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist", "smili_batch_set_start"]
 STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
           "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
           "c_gather", "c_sort", "c_scan", "c_rounds"]
@@ -138,6 +138,7 @@ def lib():
         L.smili_batch_destroy.restype = None
         L.smili_batch_profile.argtypes = [vp, C.c_int, dp, C.c_int]
         L.smili_batch_set_targets.argtypes = [vp, dp]
+        L.smili_batch_set_start.argtypes = [vp, C.c_int, dp]
         L.smili_nufft_fwd_real.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp, vp, dp, dp]
         L.smili_nufft_adj_real1d.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, vp, dp]
         _lib = L
@@ -294,6 +295,13 @@ class Batch:
         else:
             t = np.ascontiguousarray(np.broadcast_to(np.asarray(ftarget, dtype=np.float64), (self.n,)))
             check(lib().smili_batch_set_targets(self.h, dptr(t)))
+
+    def set_start(self, p, x):
+        """Problem p starts its next run from the pixel vector x (scaled units)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if x.size != self.problems[p].npix:
+            raise ValueError("start image has the wrong number of pixels")
+        check(lib().smili_batch_set_start(self.h, int(p), dptr(x)))
 
     def profile(self, enable=True):
         check(lib().smili_batch_profile(self.h, int(bool(enable)), None, 0))

@@ -1657,6 +1657,20 @@ int smili_batch_set_targets(smili_batch* b, const double* ftarget) {
   });
 }
 
+int smili_batch_set_start(smili_batch* b, int p, const double* x) {
+  return guarded([&]() -> int {
+    if (!b || p < 0 || p >= b->nprob || !x) return fail(SMILI_ERR_ARG, "invalid start-image request");
+    const ProbDesc& d = b->descs[p];
+    if (!d.o_x0 || d.nframes > 0) return fail(SMILI_ERR_UNSUPPORTED, "this problem has no replaceable start image");
+    for (int i = 0; i < d.npix; ++i)
+      if (!std::isfinite(x[i])) return fail(SMILI_ERR_DATA, "non-finite start image");
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaMemcpyAsync(b->d_arena + d.o_x0, x, sizeof(double) * d.npix, cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return SMILI_OK;
+  });
+}
+
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len) {
   return guarded([&]() -> int {
     if (!b || p < 0 || p >= b->nprob || !trace) return fail(SMILI_ERR_ARG, "invalid trace request");

@@ -253,6 +253,31 @@ def test_batched_equals_single(crescent32, closure40, lib):
     b.close()
 
 
+def test_set_start_equals_packing(crescent32, lib):
+    """A device-resident batch restarted from a new image (smili_batch_set_start)
+    solves exactly as a batch packed with that image."""
+    kw = make_kw(crescent32, niter=10)
+    x1 = np.asarray(kw["iin"]) * np.random.default_rng(3).uniform(0.5, 1.5, np.size(kw["iin"]))
+    b = lib.Batch([kw], niter=10, options=lib.make_options(64, 1e-9))
+    b.run()
+    b.set_start(0, x1)
+    b.run()
+    _, t, _, i = b.fetch(0)
+    b.close()
+    c = lib.Batch([dict(kw, iin=x1)], niter=10, options=lib.make_options(64, 1e-9))
+    c.run()
+    _, t2, _, i2 = c.fetch(0)
+    c.close()
+    assert i["niter"] == i2["niter"]
+    assert abs(t["cost"] - t2["cost"]) <= 1e-9 * abs(t2["cost"])
+    with pytest.raises(lib.SmiliError):
+        b2 = lib.Batch([kw], niter=1, options=lib.make_options(64, 1e-9))
+        try:
+            b2.set_start(0, np.full(np.size(kw["iin"]), np.nan))
+        finally:
+            b2.close()
+
+
 def test_invalid_inputs_raise(crescent32, lib):
     kw = make_kw(crescent32, niter=5)
     bad = dict(kw)
