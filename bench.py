@@ -579,7 +579,7 @@ def profile_case(case, device=0):
         w = (torch.randn(C, 3, 3, C, device=f"cuda:{device}") / 20).to(torch.bfloat16)
         y = torch.zeros(N, H, W, C, device=f"cuda:{device}", dtype=torch.bfloat16)
         out = {"case": case, "gflop": 2.0 * N * H * W * C * 9 * C / 1e9}
-        for path, name in ((0, "tcgen05"), (1, "mma_sync")):
+        for path, name in ((0, "tcgen05"), (2, "tcgen05_one_tile_per_cta"), (1, "mma_sync")):
             K.set_conv_path(path)
             for _ in range(3):
                 K.conv3x3(x, N, H, W, C, C, w, None, y, C, C, True)
@@ -704,6 +704,20 @@ def main():
     control = quality(ctl, nctl, np.arange(nctl) % S)
     control["ms"] = ctl_ms
     ctl.close()
+    # second control: FP64 from the prior with a 1e-6 relative perturbation
+    # per pixel, i.e. trajectories independent of the plain solve's after a
+    # few iterations, as FP32 trajectories are from the first evaluation on
+    rng = np.random.default_rng(7)
+    pert = [_lib.Problem(dict(kws[i % S], iin=np.asarray(kws[i % S]["iin"]) *
+                              (1.0 + 1e-6 * rng.standard_normal(np.size(kws[i % S]["iin"])))))
+            for i in range(nctl)]
+    ctl = _lib.Batch(pert, niter=args.niter, options=opt64)
+    ctl.set_targets(targets[np.arange(nctl) % S])
+    ctl_ms = ctl.run()
+    control_pert = quality(ctl, nctl, np.arange(nctl) % S)
+    control_pert["ms"] = ctl_ms
+    ctl.close()
+    del pert
 
     # launch shape: CTAs per problem from whole solves of this batch with
     # its targets (a group whose problem reaches its target takes the next
@@ -849,6 +863,7 @@ def main():
                            "nrmse_vs_truth_median": float(np.median(plain_nrmse))},
             "quality_fp32": fp32,
             "quality_fp64_control": control,
+            "quality_fp64_control_perturbed_start": control_pert,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -71,8 +71,9 @@ int smili_unet_adam(float* w, void* w16, const float* g, float* m, float* v, lon
 int smili_unet_f32_to_bf16(const float* x, void* y, long long n, void* stream);
 
 /* Convolution path (forward, data gradient and weight gradient): 0 (default)
- * tcgen05 where it applies, 1 mma.sync always.  Process-wide; for comparisons
- * and tests. */
+ * tcgen05 where it applies, 1 mma.sync always, 2 tcgen05 with one 128-pixel
+ * tile per CTA in the forward convolution (the default gives a CTA two when
+ * the image has at least 16 rows).  Process-wide; for comparisons and tests. */
 int smili_unet_set_conv_path(int path);
 
 /* Reads and clears the tcgen05 convolution's error flag (synchronous):

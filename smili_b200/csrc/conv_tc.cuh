@@ -3,7 +3,8 @@
 //
 // Implicit GEMM D[pixel][cout] = sum over (tap, cin) of X[pixel + s(tap)][cin]
 // W[cout][tap][cin] with one CTA per tile of 128 output pixels (8 rows x 16
-// columns of one image) and up to 256 output channels:
+// columns of one image), or two such tiles stacked (16 x 16 pixels, two
+// accumulators sharing each weight stage), and up to 256 output channels:
 //
 // - A (128 pixels x 16 input channels, bf16, K-major) is one TMA box of the
 //   NHWC input viewed as a 4-D tensor (C, W, H, N) at (cin0, x0 + kx - 1,
@@ -48,6 +49,8 @@ __device__ int g_tc_err;  // first error code of a bounded wait that ran out (0:
 struct Params {
   int H, W, Cin, Cout, ldy, relu, accumulate;
   int tiles_x, tiles_y;
+  int msub;     // 128-pixel sub-tiles per CTA (1 or 2): one accumulator each (the second at column
+                // tmem_cols / 2), sharing every B stage
   int ntile;    // UMMA N: output channels per CTA (multiple of 16, <= 256)
   int tmem_cols;
   int kiters;   // 9 * ceil(Cin / 16)
@@ -164,15 +167,16 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
   // 1024-byte aligned ring: STAGES A tiles, then STAGES B tiles
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(dyn_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t b_bytes = (uint32_t)p.ntile * KCH * 2;
+  const uint32_t a_bytes = A_BYTES * (uint32_t)p.msub;
   unsigned char* a_ring = base;
-  unsigned char* b_ring = base + STAGES * A_BYTES;
+  unsigned char* b_ring = base + STAGES * a_bytes;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x;
   const int tx = tile % p.tiles_x;
   const int ty = (tile / p.tiles_x) % p.tiles_y;
   const int n = tile / (p.tiles_x * p.tiles_y);
-  const int x0 = tx * TILE_W, y0 = ty * TILE_H;
+  const int x0 = tx * TILE_W, y0 = ty * TILE_H * p.msub;
   const int co0 = blockIdx.y * p.ntile;
   const int cchunks = (p.Cin + KCH - 1) / KCH;
 
@@ -207,8 +211,8 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
       }
       const int tap = k / cchunks, ci0 = (k - tap * cchunks) * KCH;
       const int ky = tap / 3, kx = tap - ky * 3;
-      mbar_expect_tx(&full_bar[s], A_BYTES + b_bytes);
-      tma_load_4d(a_ring + s * A_BYTES, &tmx, &full_bar[s], ci0, x0 + kx - 1, y0 + ky - 1, n);
+      mbar_expect_tx(&full_bar[s], a_bytes + b_bytes);
+      tma_load_4d(a_ring + s * a_bytes, &tmx, &full_bar[s], ci0, x0 + kx - 1, y0 + ky - 1, n);
       tma_load_3d(b_ring + s * b_bytes, &tmw, &full_bar[s], ci0, tap, co0);
       issued = k + 1;
     }
@@ -223,8 +227,10 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
         break;
       }
       fence_after();
-      umma_bf16(tmem, sdesc_k_sw32(smem_u32(a_ring + s * A_BYTES)), sdesc_k_sw32(smem_u32(b_ring + s * b_bytes)),
-                idesc, k > 0 ? 1u : 0u);
+      const uint64_t bdesc = sdesc_k_sw32(smem_u32(b_ring + s * b_bytes));
+      for (int sub = 0; sub < p.msub; ++sub)  // sub-tile sub: A rows 128 sub .., accumulator at column half sub
+        umma_bf16(tmem + (uint32_t)(sub * (p.tmem_cols / 2)),
+                  sdesc_k_sw32(smem_u32(a_ring + s * a_bytes + sub * A_BYTES)), bdesc, idesc, k > 0 ? 1u : 0u);
       umma_commit(&empty_bar[s]);
     }
     consumed = k;
@@ -240,16 +246,17 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
       if (!mbar_wait(&full_bar[k % STAGES], (k / STAGES) & 1)) set_err(4);
   }
 
-  // epilogue: warp w reads the accumulator rows (pixels) 32w .. 32w+31
+  // epilogue: warp w reads the accumulator rows (pixels) 32w .. 32w+31 of
+  // each sub-tile
+  const bool vec = (p.ldy % 8 == 0) && ((reinterpret_cast<uintptr_t>(p.y) & 15) == 0) && ((co0 & 7) == 0);
+  for (int sub = 0; sub < p.msub; ++sub) {
   const int r = warp * 32 + lane;
-  const int oy = y0 + r / TILE_W, ox = x0 + r % TILE_W;
+  const int oy = y0 + sub * TILE_H + r / TILE_W, ox = x0 + r % TILE_W;
   const bool in = oy < p.H && ox < p.W;
   __nv_bfloat16* dst = p.y + (((size_t)n * p.H + (in ? oy : 0)) * p.W + (in ? ox : 0)) * p.ldy;
-  // 16-byte stores when the row of output channels allows them
-  const bool vec = (p.ldy % 8 == 0) && ((reinterpret_cast<uintptr_t>(p.y) & 15) == 0) && ((co0 & 7) == 0);
   for (int c = 0; c < p.ntile; c += 16) {
     float v[16];
-    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(sub * (p.tmem_cols / 2) + c), v);
     if (!in) continue;
     if (vec && co0 + c + 16 <= p.Cout) {
       uint4 old[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
@@ -282,6 +289,7 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(const __grid_constant__
       if (p.accumulate) x += __bfloat162float(dst[co]);
       dst[co] = __float2bfloat16(x);
     }
+  }
   }
   fence_before();
   __syncthreads();
@@ -489,7 +497,9 @@ inline bool eligible(const void* x, int Cin, int ldx, const void* w, int Cout) {
          (reinterpret_cast<uintptr_t>(w) & 15) == 0 && Cout >= 1 && encode_fn() != nullptr;
 }
 
-inline size_t dyn_bytes(int ntile) { return 1024 + (size_t)STAGES * (A_BYTES + (size_t)ntile * KCH * 2); }
+inline size_t dyn_bytes(int ntile, int msub) {
+  return 1024 + (size_t)STAGES * ((size_t)A_BYTES * msub + (size_t)ntile * KCH * 2);
+}
 
 inline std::string& last_error() {
   static thread_local std::string e;
@@ -502,20 +512,24 @@ inline int fail(const std::string& msg) {
 }
 
 // returns 0 or a negative code (the reason in last_error())
+// msub_max 2 lets a CTA own two 128-pixel sub-tiles (16 x 16 pixels) that
+// share every weight stage, halving the weight traffic per flop, when the
+// image has at least 16 rows.
 inline int launch(const __nv_bfloat16* x, int N, int H, int W, int Cin, int ldx, const __nv_bfloat16* w,
                   const float* bias, __nv_bfloat16* y, int ldy, int Cout, int relu, int accumulate,
-                  cudaStream_t stream) {
+                  cudaStream_t stream, int msub_max = 2) {
   last_error().clear();
   EncodeTiledFn enc = encode_fn();
   if (!enc) return fail("cuTensorMapEncodeTiled is not available from the driver");
   const int ntile = std::min(256, (Cout + 15) / 16 * 16);
+  const int msub = (msub_max >= 2 && H >= 2 * TILE_H) ? 2 : 1;
   int cols = 32;
-  while (cols < ntile) cols *= 2;
+  while (cols < msub * ntile) cols *= 2;
   CUtensorMap mx, mw;
   {
     const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
     const cuuint64_t strides[3] = {(cuuint64_t)ldx * 2, (cuuint64_t)W * ldx * 2, (cuuint64_t)H * W * ldx * 2};
-    const cuuint32_t box[4] = {KCH, TILE_W, TILE_H, 1};
+    const cuuint32_t box[4] = {KCH, TILE_W, (cuuint32_t)(TILE_H * msub), 1};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     const CUresult r = enc(&mx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(x), dims, strides,
                            box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
@@ -541,7 +555,8 @@ inline int launch(const __nv_bfloat16* x, int N, int H, int W, int Cin, int ldx,
   p.relu = relu;
   p.accumulate = accumulate;
   p.tiles_x = (W + TILE_W - 1) / TILE_W;
-  p.tiles_y = (H + TILE_H - 1) / TILE_H;
+  p.tiles_y = (H + TILE_H * msub - 1) / (TILE_H * msub);
+  p.msub = msub;
   p.ntile = ntile;
   p.tmem_cols = cols;
   p.kiters = 9 * ((Cin + KCH - 1) / KCH);
@@ -555,7 +570,7 @@ inline int launch(const __nv_bfloat16* x, int N, int H, int W, int Cin, int ldx,
   // shared memory sized so that the CTAs one SM can hold never ask for more
   // than the SM's 512 tensor-memory columns (an allocation beyond them would
   // wait for another CTA to free its columns)
-  size_t smem = dyn_bytes(ntile);
+  size_t smem = dyn_bytes(ntile, msub);
   const size_t sm_total = 228 * 1024;                               // shared memory of one SM
   const size_t min_for_tmem = sm_total / (512 / cols + 1) + 1024;  // at most 512 / cols CTAs fit
   if (smem < min_for_tmem) smem = min_for_tmem;

@@ -418,7 +418,8 @@ __global__ void f32_to_bf16_kernel(const float* x, __nv_bfloat16* y, size_t n) {
     y[i] = __float2bfloat16(x[i]);
 }
 
-// 0: tensor-core (tcgen05) path where it applies, else mma.sync; 1: always mma.sync
+// 0: tensor-core (tcgen05) path where it applies, else mma.sync; 1: always
+// mma.sync; 2: tcgen05 with one 128-pixel tile per CTA (for comparisons)
 int g_conv_path = 0;
 
 int grid_for(size_t n, int block = 256) {
@@ -460,7 +461,8 @@ int smili_unet_conv3x3(const void* x, int N, int H, int W, int Cin, int ldx, con
   if (tiles > 0x7fffffffLL) return SMILI_UNET_ERR_ARG;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (g_conv_path != 1 && tc::eligible(x, Cin, ldx, w, Cout))
-    return tc::launch(a.x, N, H, W, Cin, ldx, a.w, bias, a.y, ldy, Cout, relu, accumulate, s) == 0
+    return tc::launch(a.x, N, H, W, Cin, ldx, a.w, bias, a.y, ldy, Cout, relu, accumulate, s,
+                      g_conv_path == 2 ? 1 : 2) == 0
                ? 0
                : SMILI_UNET_ERR_CUDA;
   if (Cout <= 8) {
@@ -580,7 +582,7 @@ int smili_unet_adam(float* w, void* w16, const float* g, float* m, float* v, lon
 }
 
 int smili_unet_set_conv_path(int path) {
-  if (path < 0 || path > 1) return SMILI_UNET_ERR_ARG;
+  if (path < 0 || path > 2) return SMILI_UNET_ERR_ARG;
   g_conv_path = path;
   return 0;
 }
