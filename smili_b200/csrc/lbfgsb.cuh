@@ -30,13 +30,18 @@
 
 typedef unsigned __int128 u128;
 
-struct LbCtx {
+// SY: the storage type of the limited-memory matrices S and Y (double in the
+// FP64 mode, float in the FP32 mode); every dot product over them
+// accumulates in FP64.
+template <typename SY>
+struct LbCtxT {
   const ProbDesc* P;
   char* base;
   GroupCtx* g;
   LbState* S;  // shared
   int n, m, lo, hi;
-  double *x, *gv, *z, *r, *d, *t, *xp, *ws, *wy;
+  double *x, *gv, *z, *r, *d, *t, *xp;
+  SY *ws, *wy;
   signed char* iwh;
   unsigned char* freef;
   unsigned long long* bkey;
@@ -48,6 +53,17 @@ struct LbCtx {
   char* dyn;      // shared scratch (the FFT buffers)
   Prof* prof;
 };
+
+// S and Y element i (column-major, n per column), widened to FP64
+template <typename SY>
+__device__ __forceinline__ double ld_ws(const LbCtxT<SY>& c, size_t i) { return (double)c.ws[i]; }
+template <typename SY>
+__device__ __forceinline__ double ld_wy(const LbCtxT<SY>& c, size_t i) { return (double)c.wy[i]; }
+template <typename SY>
+__device__ __forceinline__ void st_sy(const LbCtxT<SY>& c, size_t i, double s, double y) {
+  c.ws[i] = (SY)s;
+  c.wy[i] = (SY)y;
+}
 
 // ---------------------------------------------------------------------------
 // small dense algebra (thread 0)
@@ -290,12 +306,14 @@ __device__ __forceinline__ void reset_memory(LbState& S) {
 }
 
 // reduce acc[0..K) over the group with the ops in c.ops; result in c.red
-__device__ bool lb_reduce(LbCtx& c, const double* acc, int K) {
+template <typename SY>
+__device__ bool lb_reduce(LbCtxT<SY>& c, const double* acc, int K) {
   block_reduce_arr(acc, c.ops, K, c.red, c.scratch);
   return group_reduce(*c.g, c.red, c.ops, K);
 }
 
-__device__ void set_ops(LbCtx& c, int K, int op_default) {
+template <typename SY>
+__device__ void set_ops(LbCtxT<SY>& c, int K, int op_default) {
   for (int k = threadIdx.x; k < K; k += blockDim.x) c.ops[k] = (unsigned char)op_default;
   __syncthreads();
 }
@@ -303,7 +321,8 @@ __device__ void set_ops(LbCtx& c, int K, int op_default) {
 // ---------------------------------------------------------------------------
 // init: active() projection and state (lbfgsb.f:1004-1104, mainlb START)
 // ---------------------------------------------------------------------------
-__device__ void lb_init(LbCtx& c, const double* x0) {
+template <typename SY>
+__device__ void lb_init(LbCtxT<SY>& c, const double* x0) {
   LbState& S = *c.S;
   const ProbDesc& P = *c.P;
   if (threadIdx.x == 0) {
@@ -350,10 +369,7 @@ __device__ void lb_init(LbCtx& c, const double* x0) {
     c.iwh[i] = P.nonneg ? 0 : -1;
     c.freef[i] = 1;
     c.d[i] = 0.0;
-    for (int j = 0; j < c.m; ++j) {
-      c.ws[(size_t)j * c.n + i] = 0.0;
-      c.wy[(size_t)j * c.n + i] = 0.0;
-    }
+    for (int j = 0; j < c.m; ++j) st_sy(c, (size_t)j * c.n + i, 0.0, 0.0);
   }
   __syncthreads();
 }
@@ -408,7 +424,8 @@ __device__ __forceinline__ int bucket_of(unsigned long long k, unsigned long lon
 // lo_key) from the unordered range [r0, r1) of the bucketed arrays into cand,
 // by radix selection on 12-bit digits of the 96-bit composite (key, index).
 // Used for a bucket that holds more than SMILI_KC breakpoints.
-__device__ int select_from_range(LbCtx& c, const unsigned long long* sbk, const int* sbi, int r0,
+template <typename SY>
+__device__ int select_from_range(LbCtxT<SY>& c, const unsigned long long* sbk, const int* sbi, int r0,
                                  int r1, u128 lo_key, u128* cand, unsigned* hist) {
   __shared__ int cnt_s, vstar_s, cum_s;
   u128 prefix = 0;
@@ -492,7 +509,8 @@ __device__ int select_from_range(LbCtx& c, const unsigned long long* sbk, const 
 constexpr size_t SMILI_CAUCHY_SMEM =
     16 * SMILI_KC + 4 * SMILI_NBUCKET + 4 * 4096 +
     8 * (SMILI_MAX_WARPS * 32 + 2 * SMILI_MAX_THREADS + 4 * SMILI_MAXM_DEV * SMILI_MAXM_DEV + 5 + 4 * SMILI_MAXM_DEV);
-__device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak, int bnded,
+template <typename SY>
+__device__ void cauchy_scan(LbCtxT<SY>& c, double f1_0, const double* p0, int nbreak, int bnded,
                             const unsigned long long* sbk, const int* sbi, const int* ghist) {
   LbState& S = *c.S;
   const int m = c.m, col = S.col, col2 = 2 * col, n = c.n;
@@ -639,8 +657,8 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
         const double dibp = c.d[idx];
         vals[0] = dibp * dibp;
         for (int j = 0; j < col; ++j) {
-          const double wy_ = c.wy[(size_t)pj[j] * n + idx];
-          const double ws_ = theta * c.ws[(size_t)pj[j] * n + idx];
+          const double wy_ = ld_wy(c, (size_t)pj[j] * n + idx);
+          const double ws_ = theta * ld_ws(c, (size_t)pj[j] * n + idx);
           vals[1 + j] = dibp * wy_;
           vals[1 + col + j] = dibp * ws_;
           vals[1 + col2 + j] = te * dibp * wy_;
@@ -775,7 +793,8 @@ __device__ void cauchy_scan(LbCtx& c, double f1_0, const double* p0, int nbreak,
 }
 
 // Returns 0 on success, -1 when bmv failed (info != 0).
-__device__ int lb_cauchy(LbCtx& c) {
+template <typename SY>
+__device__ int lb_cauchy(LbCtxT<SY>& c) {
   LbState& S = *c.S;
   const ProbDesc& P = *c.P;
   const int m = c.m, n = c.n, col = S.col, col2 = 2 * col;
@@ -825,8 +844,8 @@ __device__ int lb_cauchy(LbCtx& c) {
 #pragma unroll
         for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
           if (j < col) {
-            py[j] += c.wy[(size_t)pj[j] * n + i] * neggi;
-            ps[j] += c.ws[(size_t)pj[j] * n + i] * neggi;
+            py[j] += ld_wy(c, (size_t)pj[j] * n + i) * neggi;
+            ps[j] += ld_ws(c, (size_t)pj[j] * n + i) * neggi;
           }
         }
         if (nonneg && neggi < 0.0) {
@@ -988,7 +1007,8 @@ __device__ __forceinline__ void dmma_884(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-__device__ int lb_formk(LbCtx& c) {
+template <typename SY>
+__device__ int lb_formk(LbCtxT<SY>& c) {
   LbState& S = *c.S;
   const int m = c.m, n = c.n, col = S.col;
   // entries: Fyy (a<=b), Ass (a<=b), Fsy (a,b), Asy (a,b) over physical columns
@@ -1002,8 +1022,7 @@ __device__ int lb_formk(LbCtx& c) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int ca = lane >> 2, pk = lane & 3;
   const bool cval = ca < m;  // m <= 6 < 8: one 8x8 tile per block
-  const double* wyc = c.wy + (size_t)(cval ? ca : 0) * n;
-  const double* wsc = c.ws + (size_t)(cval ? ca : 0) * n;
+  const size_t colo = (size_t)(cval ? ca : 0) * n;
   double fyy[2] = {0.0, 0.0}, fsy[2] = {0.0, 0.0}, ass[2] = {0.0, 0.0}, asy[2] = {0.0, 0.0};
   const int nchunk = (c.hi - c.lo + 3) >> 2;
   constexpr int U = 4;  // chunks in flight per warp
@@ -1014,8 +1033,8 @@ __device__ int lb_formk(LbCtx& c) {
     for (int u = 0; u < U; ++u) {
       const int i = c.lo + 4 * (q0 + u * nw) + pk;
       const bool ok = i < c.hi;  // q0 + u*nw < nchunk whenever i < hi
-      y[u] = (ok && cval) ? wyc[i] : 0.0;
-      sv[u] = (ok && cval) ? wsc[i] : 0.0;
+      y[u] = (ok && cval) ? ld_wy(c, colo + i) : 0.0;
+      sv[u] = (ok && cval) ? ld_ws(c, colo + i) : 0.0;
       fr[u] = ok && c.freef[i] != 0;
     }
 #pragma unroll
@@ -1125,7 +1144,8 @@ __device__ int lb_formk(LbCtx& c) {
 // ---------------------------------------------------------------------------
 // cmprlb + subsm (lbfgsb.f:1720-1786, 2991-3346).  Returns 0 or an error.
 // ---------------------------------------------------------------------------
-__device__ int lb_cmprlb_subsm(LbCtx& c) {
+template <typename SY>
+__device__ int lb_cmprlb_subsm(LbCtxT<SY>& c) {
   LbState& S = *c.S;
   const ProbDesc& P = *c.P;
   const int m = c.m, n = c.n, col = S.col, col2 = 2 * col;
@@ -1155,8 +1175,8 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
     double wyv[SMILI_MAXM_DEV], wsv[SMILI_MAXM_DEV];
 #pragma unroll
     for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
-      wyv[j] = j < col ? c.wy[(size_t)pj[j] * n + i] : 0.0;
-      wsv[j] = j < col ? c.ws[(size_t)pj[j] * n + i] : 0.0;
+      wyv[j] = j < col ? ld_wy(c, (size_t)pj[j] * n + i) : 0.0;
+      wsv[j] = j < col ? ld_ws(c, (size_t)pj[j] * n + i) : 0.0;
     }
     double ri;
     if (unc) {
@@ -1221,7 +1241,7 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
       double ri = c.r[i];
 #pragma unroll
       for (int j = 0; j < SMILI_MAXM_DEV; ++j)
-        if (j < col) ri += c.wy[(size_t)pj[j] * n + i] * wq[j] / theta + c.ws[(size_t)pj[j] * n + i] * wr[j];
+        if (j < col) ri += ld_wy(c, (size_t)pj[j] * n + i) * wq[j] / theta + ld_ws(c, (size_t)pj[j] * n + i) * wr[j];
       ri *= rtheta;
       c.r[i] = ri;
       if (P.nonneg) {
@@ -1293,7 +1313,8 @@ __device__ int lb_cmprlb_subsm(LbCtx& c) {
 // ---------------------------------------------------------------------------
 enum { LB_RET_DONE = 0, LB_RET_FG = 1, LB_RET_RESTART = 2, LB_RET_ABORT = -9 };
 
-__device__ int lb_abort(LbCtx& c) {
+template <typename SY>
+__device__ int lb_abort(LbCtxT<SY>& c) {
   if (threadIdx.x == 0) {
     c.S->error = 1;
     c.S->task = LB_TASK_ERROR;
@@ -1304,7 +1325,8 @@ __device__ int lb_abort(LbCtx& c) {
 }
 
 // x = t + stp d, or z when stp == 1 (lnsrlb, lbfgsb.f:2562-2570)
-__device__ void lb_set_trial_x(LbCtx& c) {
+template <typename SY>
+__device__ void lb_set_trial_x(LbCtxT<SY>& c) {
   const double stp = c.S->stp;
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x)
     c.x[i] = (stp == 1.0) ? c.z[i] : stp * c.d[i] + c.t[i];
@@ -1312,7 +1334,8 @@ __device__ void lb_set_trial_x(LbCtx& c) {
 }
 
 // "info /= 0 or iback >= 20" branch of mainlb (lbfgsb.f:888-920)
-__device__ int lb_ls_fail(LbCtx& c) {
+template <typename SY>
+__device__ int lb_ls_fail(LbCtxT<SY>& c) {
   for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
     c.x[i] = c.t[i];
     c.gv[i] = c.r[i];
@@ -1345,7 +1368,8 @@ __device__ int lb_ls_fail(LbCtx& c) {
 }
 
 // label 555 + the first part of lnsrlb (lbfgsb.f:2480-2575)
-__device__ int lb_lnsrch_start(LbCtx& c) {
+template <typename SY>
+__device__ int lb_lnsrch_start(LbCtxT<SY>& c) {
   LbState& S = *c.S;
   const bool bounded_steps = S.cnstnd && S.iter > 0;
   double acc[3] = {0.0, 1.0e10, 0.0};  // dtd, stpmx (min), gd
@@ -1408,7 +1432,8 @@ __device__ int lb_lnsrch_start(LbCtx& c) {
 }
 
 // label 222 onwards: Cauchy point, subspace minimisation, line-search start
-__device__ int lb_iter(LbCtx& c) {
+template <typename SY>
+__device__ int lb_iter(LbCtxT<SY>& c) {
   LbState& S = *c.S;
   for (int guard = 0; guard < 4; ++guard) {
     if (threadIdx.x == 0) S.iword = -1;
@@ -1468,7 +1493,8 @@ __device__ int lb_iter(LbCtx& c) {
 // Called after every function/gradient evaluation with the group-reduced
 // f, g.d and projected-gradient norm.  Returns LB_RET_FG when x holds the next
 // point to evaluate, LB_RET_DONE when the solve is over.
-__device__ int lb_after_fg(LbCtx& c, double f, double gd_fg, double sbg) {
+template <typename SY>
+__device__ int lb_after_fg(LbCtxT<SY>& c, double f, double gd_fg, double sbg) {
   LbState& S = *c.S;
   const ProbDesc& P = *c.P;
   const int m = c.m;
@@ -1584,12 +1610,11 @@ __device__ int lb_after_fg(LbCtx& c, double f, double gd_fg, double sbg) {
 #pragma unroll
       for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
         if (j < m) {
-          ay[j] += di * c.wy[(size_t)j * n + i];
-          as[j] += c.ws[(size_t)j * n + i] * di;
+          ay[j] += di * ld_wy(c, (size_t)j * n + i);
+          as[j] += ld_ws(c, (size_t)j * n + i) * di;
         }
       }
-      c.ws[(size_t)itail * n + i] = di;
-      c.wy[(size_t)itail * n + i] = ri;
+      st_sy(c, (size_t)itail * n + i, di, ri);
       c.r[i] = ri;
       c.d[i] = di;
     }

@@ -141,7 +141,7 @@ __device__ __forceinline__ void global_regs(const ProbDesc& P, const RegMoments&
 // One evaluation of a 2D problem: f, g.d, projected-gradient norm and the
 // 15 cost terms (fftim2d.f90:387-607).
 template <typename R>
-__device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsigned char* ops,
+__device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtxT<R>& lc, double* red, unsigned char* ops,
                          double* scratch, double& f, double& gd, double& sbg, double* terms,
                          int mode) {
   const ProbDesc& P = *fc.P;
@@ -190,7 +190,7 @@ __device__ bool group_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsi
 // iz < Nz as the reference does) and forms g.d and the projected gradient
 // over the whole vector.  terms[20] follow the fftim3d.imaging order.
 template <typename R>
-__device__ bool movie_fg(FgCtx<R>& fc, GroupCtx& g, LbCtx& lc, double* red, unsigned char* ops,
+__device__ bool movie_fg(FgCtx<R>& fc, GroupCtx& g, LbCtxT<R>& lc, double* red, unsigned char* ops,
                          double* scratch, double& f, double& gd, double& sbg, double* terms) {
   const ProbDesc& M = *fc.P;
   char* base = fc.base;
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(Shape<R>::threads, Shape<R>::min_blocks) smili
     fc.swork = fc.sbuf + SMILI_SMEM_CPX;
     fc.smem_cpx = SMILI_SMEM_CPX;
     fc.dyn_cpx = SMILI_DYN_CPX;
-    LbCtx lc;
+    LbCtxT<R> lc;
     lc.P = &P;
     lc.base = base;
     lc.g = &g;
@@ -367,8 +367,8 @@ __global__ void __launch_bounds__(Shape<R>::threads, Shape<R>::min_blocks) smili
     lc.d = at<double>(base, P.o_d);
     lc.t = at<double>(base, P.o_t);
     lc.xp = at<double>(base, P.o_xp);
-    lc.ws = at<double>(base, P.o_ws);
-    lc.wy = at<double>(base, P.o_wy);
+    lc.ws = at<R>(base, P.o_ws);  // S and Y in the kernel's precision
+    lc.wy = at<R>(base, P.o_wy);
     lc.iwh = at<signed char>(base, P.o_iwh);
     lc.freef = at<unsigned char>(base, P.o_free);
     lc.bkey = at<unsigned long long>(base, P.o_bkey);
@@ -940,9 +940,9 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.o_lred = ar.take(sizeof(double) * 64);
     d.o_trace = ar.take(sizeof(double) * (niter + 2));
   }
-  if (kind == PK_SOLVE) {
-    d.o_ws = ar.take(sizeof(double) * (size_t)N * m);
-    d.o_wy = ar.take(sizeof(double) * (size_t)N * m);
+  if (kind == PK_SOLVE) {  // S and Y: R per element (FP32 storage in the FP32 mode)
+    d.o_ws = ar.take(sizeof(R) * (size_t)N * m);
+    d.o_wy = ar.take(sizeof(R) * (size_t)N * m);
   }
   // ---- blobs ----
   if (!frame) hp.put(d.o_x0, std::vector<double>(x0, x0 + N));
@@ -1373,9 +1373,9 @@ int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, i
   d.o_hist = ar.take(sizeof(int) * 2 * 4096);
   d.o_lred = ar.take(sizeof(double) * 64);
   d.o_trace = ar.take(sizeof(double) * (niter + 2));
-  if (kind == PK_SOLVE) {
-    d.o_ws = ar.take(sizeof(double) * (size_t)n * m);
-    d.o_wy = ar.take(sizeof(double) * (size_t)n * m);
+  if (kind == PK_SOLVE) {  // S and Y: R per element (FP32 storage in the FP32 mode)
+    d.o_ws = ar.take(sizeof(R) * (size_t)n * m);
+    d.o_wy = ar.take(sizeof(R) * (size_t)n * m);
   }
   d.o_frames = ar.take(sizeof(ProbDesc) * Nz);
   d.o_lcf = ar.take(sizeof(double) * Nz);
