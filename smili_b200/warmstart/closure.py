@@ -15,7 +15,7 @@ the network maps it to the plain method's converged image.
   same L-BFGS-B with the remaining iteration budget.  The plain FP64 solve's
   final cost stays the judge: a solve counts when it reaches it.
 
-    python -m smili_b200.warmstart.closure --ntrain 768 --out unet_closure256.npz
+    python -m smili_b200.warmstart.closure --ntrain 2048 --workers 8 --out unet_closure256.npz
 """
 from __future__ import annotations
 
@@ -44,6 +44,27 @@ def make_set(seeds, niter=1000):
                                 niter=niter, **obs.reg)
         out.append((kw, obs.truth, obs.totalflux))
     return out
+
+
+def _make_chunk(args):
+    seeds, niter = args
+    return make_set(seeds, niter)
+
+
+def make_set_parallel(seeds, niter=1000, workers=1):
+    """``make_set`` over host worker processes (started with spawn; each
+    computes its model visibilities on the GPU)."""
+    seeds = list(seeds)
+    if workers <= 1 or len(seeds) < 2 * workers:
+        return make_set(seeds, niter)
+    import multiprocessing as mp
+    parts = [seeds[i::workers] for i in range(workers)]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        done = pool.map(_make_chunk, [(part, niter) for part in parts])
+    by_seed = {}
+    for part, res in zip(parts, done):
+        by_seed.update(zip(part, res))
+    return [by_seed[s] for s in seeds]
 
 
 def normalise(imgs):
@@ -106,22 +127,34 @@ def main(argv=None):
     ap.add_argument("--rtol", type=float, default=1e-4)
     ap.add_argument("--out", default="unet_closure256.npz")
     ap.add_argument("--report", default=None)
+    ap.add_argument("--workers", type=int, default=1, help="host processes that make the training problems")
+    ap.add_argument("--chunk", type=int, default=512, help="training problems made and solved at a time")
     args = ap.parse_args(argv)
 
     def log(msg):
         print(f"[{time.strftime('%H:%M:%S')}] {msg}", flush=True)
 
     rep = {"args": vars(args)}
-    t0 = time.time()
-    tr = make_set(range(20000, 20000 + args.ntrain), args.niter)
-    kws = [e[0] for e in tr]
-    rep["t_generate_s"] = time.time() - t0
-    log(f"generated {len(tr)} problems in {rep['t_generate_s']:.0f} s")
-    _, X, _, ms_k = early_images(kws, args.K)
-    xs, _, _, _, ms_p = data.solve(kws, args.niter, 64, chunk=256)
-    Y = normalise([data.to_grid(kw, x) for kw, x in zip(kws, xs)])
-    rep["plain_fp64_batched_s"] = ms_p / 1000.0
-    log(f"early images {ms_k / 1000:.1f} s, plain FP64 solves {ms_p / 1000:.1f} s on the device")
+    X, Y = [], []
+    t_gen = ms_k = ms_p = 0.0
+    for c0 in range(0, args.ntrain, args.chunk):  # pairs made a chunk at a time: only images are kept
+        t0 = time.time()
+        tr = make_set_parallel(range(20000 + c0, 20000 + min(args.ntrain, c0 + args.chunk)), args.niter,
+                               args.workers)
+        kws = [e[0] for e in tr]
+        t_gen += time.time() - t0
+        _, xk, _, ms = early_images(kws, args.K)
+        ms_k += ms
+        xs, _, _, _, ms = data.solve(kws, args.niter, 64, chunk=256)
+        ms_p += ms
+        X.append(xk)
+        Y.append(normalise([data.to_grid(kw, x) for kw, x in zip(kws, xs)]))
+        del tr, kws, xs
+        log(f"training pairs {min(args.ntrain, c0 + args.chunk)}/{args.ntrain}")
+    X, Y = np.concatenate(X), np.concatenate(Y)
+    rep["t_generate_s"], rep["plain_fp64_batched_s"] = t_gen, ms_p / 1000.0
+    log(f"generation {t_gen:.0f} s; early images {ms_k / 1000:.1f} s, plain FP64 solves {ms_p / 1000:.1f} s "
+        "on the device")
     net = UNet(seed=0)
     t0 = time.time()
     rep["losses"] = train(net, X, Y, args.epochs, args.batch, args.lr, log=log)

@@ -51,3 +51,44 @@ def test_warm_start_beats_gaussian_prior(net):
     assert it_warm.mean() <= 0.9 * it_plain.mean()
     assert nr_0 < nr_g          # the proposal itself is closer to the truth than the prior
     assert nr_w <= nr_p * 1.05  # and the final image is as good as the plain one
+
+
+WEIGHTS_CLOSURE = os.path.join(os.path.dirname(os.path.dirname(__file__)), "smili_b200", "warmstart",
+                               "unet_closure256.npz")
+
+
+def test_closure_warm_start_moves_toward_the_plain_solution():
+    """The 256x256 closure-data warm start (amplitudes, closure phases, log
+    closure amplitudes; smili_b200/warmstart/closure.py) on 8 held-out seeds:
+    the network's proposal from the image after 50 FP32 iterations is closer
+    (median NRMSE) to the plain FP64 solve's final image than that 50-
+    iteration image itself, and starting the remaining FP32 iterations from
+    it reaches the plain final cost at least as often as the cold FP32 solve
+    minus one."""
+    from smili_b200.warmstart import closure, data
+    from smili_b200.warmstart.unet import UNet
+    if not os.path.exists(WEIGHTS_CLOSURE):
+        pytest.fail(f"trained weights missing: {WEIGHTS_CLOSURE}")
+    net = UNet.load(WEIGHTS_CLOSURE)
+    niter = 1000
+    ev = closure.make_set(range(40000, 40008), niter)
+    kws = [e[0] for e in ev]
+    xs_p, _, cost_p, _, _ = data.solve(kws, niter, 64)
+    targets = cost_p * (1 + 1e-4)
+    xk, imk, ik, _ = closure.early_images(kws, closure.K_DEFAULT)
+    pred = net.predict(imk)
+    assert np.all(np.isfinite(pred))
+    plain = closure.normalise([data.to_grid(kw, x) for kw, x in zip(kws, xs_p)])
+    nr_k = np.median([data.nrmse(a, b) for a, b in zip(imk, plain)])
+    nr_p = np.median([data.nrmse(closure.normalise([np.maximum(p, 0)])[0], b) for p, b in zip(pred, plain)])
+    x0 = [closure.warm_init(kw, p, x) for kw, p, x in zip(kws, pred, xk)]
+    assert all(np.all(np.isfinite(x)) and np.all(x >= 0) for x in x0)
+    assert all(abs(np.sum(a) - np.sum(b)) <= 1e-6 * np.sum(b) for a, b in zip(x0, xk))  # flux kept
+    _, icold, _, _, _ = data.solve(kws, niter, 32, targets=targets)
+    _, iw, _, _, _ = data.solve(kws, niter - closure.K_DEFAULT, 32, targets=targets, x0=x0)
+    cold = sum(i["task"] == 8 for i in icold)
+    warm = sum(a["task"] == 8 or b["task"] == 8 for a, b in zip(ik, iw))
+    print(f"NRMSE to the plain image: 50-iteration {nr_k:.3f}, proposal {nr_p:.3f}; reached cold {cold}/8 "
+          f"warm {warm}/8")
+    assert nr_p < nr_k
+    assert warm >= cold - 1
