@@ -283,17 +283,18 @@ UNET_FORWARD_LAUNCHES = 21  # 15 convolutions, 3 poolings, 3 upsamplings per for
 class WarmStart:
     """The learned warm start on this workload (``smili_b200.warmstart.closure``).
 
-    One step: K FP32 iterations of every problem from its prior (one
-    launch), the U-Net's proposal from each K-iteration image, then the
-    remaining niter - K FP32 iterations from the proposals (a second launch
-    of the same device-resident problems, restarted with
-    ``Batch.set_start``), with the same targets as the cold arm.  A problem
-    that reaches its target in the first K iterations counts there and
-    restarts from its own image.  The step's time is the two launches' CUDA
-    event times, the network's forward pass (CUDA events) and the host work
-    between them (fetching the K-iteration images, forming the network
-    input, turning its output into starting vectors and uploading them;
-    wall clock)."""
+    One step: K FP32 iterations of every problem from its prior, the U-Net's
+    proposal from each K-iteration image, then the remaining niter - K FP32
+    iterations from the proposals, with the same targets as the cold arm.
+    Both phases are launches of one device-resident batch: between them
+    ``Batch.set_niter`` changes the iteration caps and ``Batch.set_start``
+    replaces the start images (the priors are put back at the start of the
+    next step).  A problem that reaches its target in the first K
+    iterations counts there and restarts from its own image.  The step's
+    time is the two launches' CUDA event times, the network's forward pass
+    (CUDA events) and the host work around them (restoring the priors,
+    fetching the K-iteration images, forming the network input, turning its
+    output into starting vectors and uploading them; wall clock)."""
 
     def __init__(self, probs, kws, seed_of, ftarget, niter, G, device=0):
         import torch
@@ -302,24 +303,27 @@ class WarmStart:
         from smili_b200.warmstart.unet import UNet
         self.torch, self.lib, self.closure = torch, _lib, closure
         self.net = UNet.load(WARM_WEIGHTS, device=f"cuda:{device}")
-        self.K = closure.K_DEFAULT
+        self.K, self.niter = closure.K_DEFAULT, niter
         self.kws, self.seed_of, self.B = kws, seed_of, len(probs)
-        self.opts = _lib.make_options(32, 1e-6, G, device)
-        self.bk = _lib.Batch(probs, niter=self.K, options=self.opts)
-        self.bk.set_targets(ftarget)
-        self.bw = _lib.Batch(probs, niter=niter - self.K, options=self.opts)
-        self.bw.set_targets(ftarget)
+        self.prior = [np.asarray(kws[s]["iin"], dtype=np.float64) for s in seed_of]
+        self.b = _lib.Batch(probs, niter=niter, options=_lib.make_options(32, 1e-6, G, device))
+        self.b.set_targets(ftarget)
         nx = int(kws[0]["nx"])
         self.net.predict(np.zeros((self.B, nx, nx), np.float32), batch=self.B)  # buffers and first-call set-up
 
     def step(self):
         from smili_b200.warmstart import data
-        torch, _lib, closure, B = self.torch, self.lib, self.closure, self.B
-        ms_k = self.bk.run()
+        torch, _lib, closure, B, b = self.torch, self.lib, self.closure, self.B, self.b
         t0 = time.perf_counter()
-        early = [self.bk.fetch(p) for p in range(B)]
-        imgs = closure.normalise([data.to_grid(self.kws[self.seed_of[p]], early[p][0]) for p in range(B)])
+        b.set_niter(self.K)
+        for p in range(B):
+            b.set_start(p, self.prior[p])
         t_host = time.perf_counter() - t0
+        ms_k = b.run()
+        t0 = time.perf_counter()
+        early = [b.fetch(p) for p in range(B)]
+        imgs = closure.normalise([data.to_grid(self.kws[self.seed_of[p]], early[p][0]) for p in range(B)])
+        t_host += time.perf_counter() - t0
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         pred = self.net.predict(imgs, batch=B)
@@ -329,10 +333,11 @@ class WarmStart:
         hit_k = np.array([e[3]["task"] == _lib.TASK_TARGET for e in early])
         for p in range(B):
             x0 = early[p][0] if hit_k[p] else closure.warm_init(self.kws[self.seed_of[p]], pred[p], early[p][0])
-            self.bw.set_start(p, x0)
+            b.set_start(p, x0)
+        b.set_niter(self.niter - self.K)
         t_host += time.perf_counter() - t0
-        ms_w = self.bw.run()
-        infos = [self.bw.fetch(p)[3] for p in range(B)]
+        ms_w = b.run()
+        infos = [b.fetch(p)[3] for p in range(B)]
         hit = hit_k | np.array([i["task"] == _lib.TASK_TARGET for i in infos])
         ms_net = e0.elapsed_time(e1)
         return {"s": (ms_k + ms_net + ms_w) / 1000.0 + t_host, "hits": int(hit.sum()),
@@ -343,11 +348,10 @@ class WarmStart:
                             "host": t_host, "remaining_iterations_device": ms_w / 1000.0}}
 
     def fetch(self, p):
-        return self.bw.fetch(p)
+        return self.b.fetch(p)
 
     def close(self):
-        self.bk.close()
-        self.bw.close()
+        self.b.close()
 
 
 WARM_WEIGHTS = os.path.join(ROOT, "smili_b200", "warmstart", "unet_closure256.npz")
@@ -785,9 +789,9 @@ def main():
         fp32["parts_s"] = {k: float(np.mean([r["parts_s"][k] for r in steps])) for k in steps[0]["parts_s"]}
         ws.close()
         launches = UNET_FORWARD_LAUNCHES + 2
-        # end to end from host buffers: packing and upload of both launches'
-        # problems, the step (its start images uploaded inside), download
-        h2d = 2 * h2d_prob + 8 * npix_all
+        # end to end from host buffers: packing and upload of the problems,
+        # the step (start images uploaded twice inside), download
+        h2d = h2d_prob + 2 * 8 * npix_all
         d2h = 2 * (2 * 8 * npix_all + 15 * 8 * B) + 8 * npix_all
     else:
         ms_step, kernel_s = cold["ms_per_step"], cold["ms_per_step"] / 1000.0

@@ -128,6 +128,12 @@ int smili_batch_set_targets(smili_batch* b, const double* ftarget);
  * a device-resident batch from new images (a warm start) without packing
  * and uploading its data again.  Movies are not supported. */
 int smili_batch_set_start(smili_batch* b, int p, const double* x);
+
+/* Change the iteration caps of the next runs (no reference counterpart):
+ * niter[p] between 0 and the cap problem p was created with; NULL restores
+ * those caps.  With smili_batch_set_start this lets one device-resident
+ * batch run a few iterations, restart from new images and run the rest. */
+int smili_batch_set_niter(smili_batch* b, const int* niter);
 /* Cost recorded at each completed iteration of problem p (NaN where absent). */
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len);
 void smili_batch_destroy(smili_batch* b);

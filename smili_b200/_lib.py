@@ -105,7 +105,7 @@ EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "sm
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
            "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile",
            "smili_batch_set_targets", "smili_calc_cost_noalloc", "smili_fftim3d_imaging",
-           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist", "smili_batch_set_start"]
+           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist", "smili_batch_set_start", "smili_batch_set_niter"]
 STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
           "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
           "c_gather", "c_sort", "c_scan", "c_rounds"]
@@ -139,6 +139,7 @@ def lib():
         L.smili_batch_profile.argtypes = [vp, C.c_int, dp, C.c_int]
         L.smili_batch_set_targets.argtypes = [vp, dp]
         L.smili_batch_set_start.argtypes = [vp, C.c_int, dp]
+        L.smili_batch_set_niter.argtypes = [vp, ip]
         L.smili_nufft_fwd_real.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp, vp, dp, dp]
         L.smili_nufft_adj_real1d.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, vp, dp]
         _lib = L
@@ -295,6 +296,14 @@ class Batch:
         else:
             t = np.ascontiguousarray(np.broadcast_to(np.asarray(ftarget, dtype=np.float64), (self.n,)))
             check(lib().smili_batch_set_targets(self.h, dptr(t)))
+
+    def set_niter(self, niter):
+        """Iteration caps of the next runs (each at most the cap at creation); None restores them."""
+        if niter is None:
+            check(lib().smili_batch_set_niter(self.h, None))
+        else:
+            n = np.ascontiguousarray(np.broadcast_to(np.asarray(niter, dtype=np.int32), (self.n,)))
+            check(lib().smili_batch_set_niter(self.h, n.ctypes.data_as(C.POINTER(C.c_int))))
 
     def set_start(self, p, x):
         """Problem p starts its next run from the pixel vector x (scaled units)."""

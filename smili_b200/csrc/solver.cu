@@ -1015,6 +1015,7 @@ struct smili_batch {
   bool own_stream = false;
   size_t dyn_bytes = 0;
   int profile = 0;
+  std::vector<int> niter_cap;  // iteration caps at packing (trace buffers are sized for them)
 };
 
 namespace {
@@ -1140,6 +1141,8 @@ int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smi
                  smili_batch** out) {
   const int device = b->device;
   const int nprob = b->nprob;
+  b->niter_cap.clear();
+  for (const ProbDesc& d : b->descs) b->niter_cap.push_back(d.niter);
   // inputs are valid: now the device
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) {
@@ -1649,6 +1652,24 @@ int smili_batch_set_targets(smili_batch* b, const double* ftarget) {
   return guarded([&]() -> int {
     if (!b) return fail(SMILI_ERR_ARG, "null batch");
     for (int p = 0; p < b->nprob; ++p) b->descs[p].ftarget = ftarget ? ftarget[p] : -INFINITY;
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaMemcpyAsync(b->d_descs, b->descs.data(), sizeof(ProbDesc) * b->nprob, cudaMemcpyHostToDevice,
+                             b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return SMILI_OK;
+  });
+}
+
+int smili_batch_set_niter(smili_batch* b, const int* niter) {
+  return guarded([&]() -> int {
+    if (!b) return fail(SMILI_ERR_ARG, "null batch");
+    if ((int)b->niter_cap.size() != b->nprob) return fail(SMILI_ERR_ARG, "batch has no iteration caps");
+    for (int p = 0; p < b->nprob; ++p) {
+      const int v = niter ? niter[p] : b->niter_cap[p];
+      if (v < 0 || v > b->niter_cap[p])
+        return fail(SMILI_ERR_ARG, "niter must lie between 0 and the iteration cap the batch was created with");
+    }
+    for (int p = 0; p < b->nprob; ++p) b->descs[p].niter = niter ? niter[p] : b->niter_cap[p];
     CUDA_TRY(cudaSetDevice(b->device));
     CUDA_TRY(cudaMemcpyAsync(b->d_descs, b->descs.data(), sizeof(ProbDesc) * b->nprob, cudaMemcpyHostToDevice,
                              b->stream));

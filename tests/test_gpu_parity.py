@@ -278,6 +278,28 @@ def test_set_start_equals_packing(crescent32, lib):
             b2.close()
 
 
+def test_set_niter_equals_packing(crescent32, lib):
+    """Lowered iteration caps (smili_batch_set_niter) solve as a batch packed
+    with them; caps above the packed ones are refused; None restores them."""
+    kw = make_kw(crescent32, niter=12)
+    b = lib.Batch([kw], niter=12, options=lib.make_options(64, 1e-9))
+    b.set_niter(5)
+    b.run()
+    _, t, _, i = b.fetch(0)
+    c = lib.Batch([dict(kw, niter=5)], niter=5, options=lib.make_options(64, 1e-9))
+    c.run()
+    _, t2, _, i2 = c.fetch(0)
+    c.close()
+    assert i["niter"] == i2["niter"] == 6
+    assert abs(t["cost"] - t2["cost"]) <= 1e-9 * abs(t2["cost"])
+    with pytest.raises(lib.SmiliError):
+        b.set_niter(13)
+    b.set_niter(None)
+    b.run()
+    assert b.fetch(0)[3]["niter"] == 13
+    b.close()
+
+
 def test_invalid_inputs_raise(crescent32, lib):
     kw = make_kw(crescent32, niter=5)
     bad = dict(kw)
