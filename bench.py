@@ -540,6 +540,8 @@ def profile_case(case, device=0):
 
     - ``traffic``: the benchmark's concurrency (74 resident groups of 4 CTAs,
       74 problems of the workload) for 20 FP32 iterations;
+    - ``stages``: the same launch with the stage profiler on, every group busy
+      for the whole launch: the steady-state time split per evaluation;
     - ``fg``: one FP32 function/gradient evaluation of those 74 problems;
     - ``t2`` / ``t1``: one FP32 type-2 / type-1 transform of the workload's
       97 200 uv points on the 256 x 256 grid (the transform stages alone);
@@ -549,21 +551,32 @@ def profile_case(case, device=0):
     Inputs come from the library's own transform (fast), not the exact DFT."""
     from smili_b200 import _lib, synth
     from smili_b200.imaging.lbfgs import prepare_imaging
-    if case in ("traffic", "fg", "t2", "t1"):
+    if case in ("traffic", "stages", "fg", "t2", "t1"):
         kws = []
-        for s in range(16 if case in ("traffic", "fg") else 1):
+        for s in range(16 if case in ("traffic", "stages", "fg") else 1):
             obs = synth.precision_path(seed=1000 + s, niter=20, model=synth.nufft_model)
             kw, _ = prepare_imaging(obs.image, amptable=obs.amptable, bstable=obs.bstable,
                                     catable=obs.catable, niter=20, **obs.reg)
             kws.append(kw)
-    if case in ("traffic", "fg"):
+    if case in ("traffic", "stages", "fg"):
         P = [_lib.Problem(k) for k in kws]
-        b = _lib.Batch([P[i % 16] for i in range(74)], niter=20 if case == "traffic" else 1,
+        b = _lib.Batch([P[i % 16] for i in range(74)], niter=1 if case == "fg" else 20,
                        options=_lib.make_options(32, 1e-6, 4, device))
+        if case == "stages":
+            b.run()  # warm-up
+            b.profile(True)
         ms = b.run(fg_only=case == "fg")
         nfg = sum(b.fetch(p)[3]["nfg"] for p in range(74))
+        out = {"case": case, "ms": ms, "evaluations": nfg}
+        if case == "stages":
+            st = b.stage_times()
+            n0 = st.pop("n_fg")
+            out["group0_us_per_evaluation"] = {k: round(1000.0 * v / n0, 1) for k, v in st.items()
+                                               if k != "c_rounds"}
+            out["group0_evaluations"] = n0
+            b.profile(False)
         b.close()
-        print(json.dumps({"case": case, "ms": ms, "evaluations": nfg}))
+        print(json.dumps(out))
     elif case in ("t2", "t1"):
         from smili_b200.fortlib import fftlib
         u, v = np.asarray(kws[0]["u"]), np.asarray(kws[0]["v"])
@@ -627,7 +640,7 @@ def main():
                     help="time the cold arm (prior starts) as the headline instead of the learned warm start")
     ap.add_argument("--warm-problems", type=int, default=256,
                     help="held-out problems of the learned warm-start comparison (0: skip)")
-    ap.add_argument("--case", default=None, choices=["traffic", "fg", "t2", "t1", "conv"],
+    ap.add_argument("--case", default=None, choices=["traffic", "stages", "fg", "t2", "t1", "conv"],
                     help="run one small launch for a profiler capture instead of the benchmark")
     args = ap.parse_args()
     if args.case:

@@ -41,6 +41,7 @@ __device__ __forceinline__ int imod(int a, int n) {
 __device__ __forceinline__ int wrapn(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
 
 __device__ __forceinline__ double smabs(double x) { return sqrt(x * x + 1e-10); }
+__device__ __forceinline__ float smabs(float x) { return sqrtf(x * x + 1e-10f); }
 
 // rows (sequences) per CTA pass for an FFT of length n
 __device__ __forceinline__ int fft_batch(int n) {
@@ -397,7 +398,8 @@ __device__ void fg_t2_cols(FgCtx<R>& c, const GroupCtx& g) {
 // registers and the W row loads of a tap row issue back to back.
 template <int W, typename R>
 __device__ __forceinline__ void interp_points(const ProbDesc& P, const R* __restrict__ xu, const R* __restrict__ xv,
-                                              const cpx<R>* bandA, cpx<R>* V, R beta, int j0, int dj) {
+                                              const cpx<R>* bandA, cpx<R>* V, cpx<R>* cacc, R beta, int j0,
+                                              int dj) {
   const R half = (R)0.5 * (R)W;
   const R inv = (R)1 / half;
   for (int j = j0; j < P.nuv; j += dj) {
@@ -429,19 +431,22 @@ __device__ __forceinline__ void interp_points(const ProbDesc& P, const R* __rest
       ai += k2[b] * ri;
     }
     V[j] = cmk(ar, ai);
+    if (cacc) cacc[j] = cmk<R>(0, 0);
   }
 }
 
 // ---------------------------------------------------------------------------
-// F3: type-2 interpolation, V_j = sum psi psi bandA
+// F3: type-2 interpolation, V_j = sum psi psi bandA.  With zero_acc it also
+// clears the points' derivative accumulators that F4 adds into.
 // ---------------------------------------------------------------------------
 template <typename R>
-__device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
+__device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g, bool zero_acc) {
   const ProbDesc& P = *c.P;
   const R* xu = at<R>(c.base, P.o_u);
   const R* xv = at<R>(c.base, P.o_v);
   const cpx<R>* gband = at<cpx<R>>(c.base, P.o_bandA);
   cpx<R>* V = at<cpx<R>>(c.base, P.o_V);
+  cpx<R>* cacc = zero_acc ? at<cpx<R>>(c.base, P.o_contrib) : nullptr;
   const int w = P.w;
   const R beta = (R)P.beta;
   const int ncell = P.b1n * P.b2n;
@@ -459,20 +464,33 @@ __device__ void fg_interp(FgCtx<R>& c, const GroupCtx& g) {
   const int j0 = g.rank * blockDim.x + threadIdx.x, dj = g.G * blockDim.x;
   switch (w) {
 #define SMILI_INTERP_W(W) \
-  case W: interp_points<W>(P, xu, xv, bandA, V, beta, j0, dj); break;
+  case W: interp_points<W>(P, xu, xv, bandA, V, cacc, beta, j0, dj); break;
     SMILI_INTERP_W(2) SMILI_INTERP_W(3) SMILI_INTERP_W(4) SMILI_INTERP_W(5) SMILI_INTERP_W(6)
     SMILI_INTERP_W(7) SMILI_INTERP_W(8) SMILI_INTERP_W(9) SMILI_INTERP_W(10) SMILI_INTERP_W(11)
     SMILI_INTERP_W(12) SMILI_INTERP_W(13) SMILI_INTERP_W(14) SMILI_INTERP_W(15)
-    default: interp_points<16>(P, xu, xv, bandA, V, beta, j0, dj); break;  // w <= SMILI_MAXW = 16
+    default: interp_points<16>(P, xu, xv, bandA, V, cacc, beta, j0, dj); break;  // w <= SMILI_MAXW = 16
 #undef SMILI_INTERP_W
   }
   __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
-// F4: chi-square terms and their derivatives per contribution slot.
+// F4: chi-square terms, and their derivatives with respect to each model
+// visibility added into that uv point's accumulator (o_contrib, zeroed by F3)
+// with global atomics: one vector reduction per contribution in FP32, two in
+// FP64.  The accumulators (one complex value per uv point) are small enough
+// to stay in L2 while the data stream past, and spreading then reads them in
+// its own point order.
 // chi[0..3] = fcv, amp, cp, ca (weighted by the normalised data weights).
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void acc_add(cpx<float>* p, cpx<float> v) {
+  atomicAdd(reinterpret_cast<float2*>(p), make_float2(v.x, v.y));
+}
+__device__ __forceinline__ void acc_add(cpx<double>* p, cpx<double> v) {
+  atomicAdd(&p->x, v.x);
+  atomicAdd(&p->y, v.y);
+}
+
 template <typename R>
 __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
   const ProbDesc& P = *c.P;
@@ -482,7 +500,7 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
   const R* dvar = at<R>(c.base, P.o_dvar);
   const int* didx = at<int>(c.base, P.o_didx);
   const signed char* dsgn = at<signed char>(c.base, P.o_dsgn);
-  cpx<R>* contrib = at<cpx<R>>(c.base, P.o_contrib);
+  cpx<R>* cacc = at<cpx<R>>(c.base, P.o_contrib);
   typedef typename std::conditional<sizeof(R) == 8, KSum, KSumF>::type Acc;
   Acc acc[4];
   for (int q = 0; q < 4; ++q) acc[q].s = acc[q].c = 0;
@@ -505,11 +523,11 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
     }
   };
   // complex visibilities (fftlib.f90:384-439)
-  auto fcv = [&](int i, const cpx<R>& Vk, R sg, R var, R yr, R yi) {
+  auto fcv = [&](int i, int k, const cpx<R>& Vk, R sg, R var, R yr, R yi) {
     const R rr = yr - Vk.x, ri = yi - sg * Vk.y;
     acc[0].add(((rr * rr + ri * ri) / var) * wf);
     const R factor = (R)-2 / var * wf;
-    contrib[i] = cmk(factor * rr, factor * ri * sg);
+    acc_add(cacc + k, cmk(factor * rr, factor * ri * sg));
     put(i, Vk.x, sg * Vk.y, rr, ri);
   };
   for (int i = first(0); i < e_amp; i += 2 * dj) {
@@ -520,17 +538,16 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
     const R sa = (R)dsgn[i], sb = two ? (R)dsgn[ib] : sa;
     const R va = dvar[i], vb = two ? dvar[ib] : va;
     const R ra = dre[i], rb = two ? dre[ib] : ra, ia = dim[i], ibm = two ? dim[ib] : ia;
-    fcv(i, Va, sa, va, ra, ia);
-    if (two) fcv(ib, Vb, sb, vb, rb, ibm);
+    fcv(i, ka, Va, sa, va, ra, ia);
+    if (two) fcv(ib, kb, Vb, sb, vb, rb, ibm);
   }
   // amplitudes (fftlib.f90:442-493)
-  auto amp = [&](int i, const cpx<R>& Vk, R var, R y) {
-    const int slot = s_amp + (i - e_amp);
+  auto amp = [&](int i, int k, const cpx<R>& Vk, R var, R y) {
     const R model = sqrt(Vk.x * Vk.x + Vk.y * Vk.y);
     const R resid = y - model;
     acc[1].add((resid * resid / var) * wa);
     const R factor = (R)-2 * resid / var / model * wa;
-    contrib[slot] = cmk(factor * Vk.x, factor * Vk.y);
+    acc_add(cacc + k, cmk(factor * Vk.x, factor * Vk.y));
     put(i, model, 0, resid, 0);
   };
   for (int i = first(e_amp); i < e_cp; i += 2 * dj) {
@@ -540,12 +557,11 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
     const cpx<R> Va = V[ka], Vb = V[kb];
     const R va = dvar[i], vb = two ? dvar[ib] : va;
     const R ya = dre[i], yb = two ? dre[ib] : ya;
-    amp(i, Va, va, ya);
-    if (two) amp(ib, Vb, vb, yb);
+    amp(i, ka, Va, va, ya);
+    if (two) amp(ib, kb, Vb, vb, yb);
   }
   // closure phases (fftlib.f90:576-655)
-  auto cp = [&](int i, const cpx<R> (&Vq)[3], const R (&sg)[3], R var, R y) {
-    const int slot = s_cp + 3 * (i - e_cp);
+  auto cp = [&](int i, const int (&kq)[3], const cpx<R> (&Vq)[3], const R (&sg)[3], R var, R y) {
     R a2[3];
     R model = 0;
 #pragma unroll
@@ -570,7 +586,7 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
     const R factor = (R)-2 * sr / var * wc;
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-      contrib[slot + q] = cmk(-factor / a2[q] * Vq[q].y * sg[q], factor / a2[q] * Vq[q].x * sg[q]);
+      acc_add(cacc + kq[q], cmk(-factor / a2[q] * Vq[q].y * sg[q], factor / a2[q] * Vq[q].x * sg[q]));
     put(i, model, 0, resid, 0);  // unwrapped; the host wraps both into (-pi, pi] as model_cp does
   };
   for (int i = first(e_cp); i < e_ca; i += 2 * dj) {
@@ -594,12 +610,11 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
     }
     const R va = dvar[i], vb = two ? dvar[ib] : va;
     const R ya = dre[i], yb = two ? dre[ib] : ya;
-    cp(i, Va, ga, va, ya);
-    if (two) cp(ib, Vb, gb, vb, yb);
+    cp(i, ka, Va, ga, va, ya);
+    if (two) cp(ib, kb, Vb, gb, vb, yb);
   }
   // log closure amplitudes (fftlib.f90:496-573)
-  auto ca = [&](int i, const cpx<R> (&Vq)[4], R var, R y) {
-    const int slot = s_ca + 4 * (i - e_ca);
+  auto ca = [&](int i, const int (&kq)[4], const cpx<R> (&Vq)[4], R var, R y) {
     R a[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) a[q] = sqrt(Vq[q].x * Vq[q].x + Vq[q].y * Vq[q].y);
@@ -610,7 +625,7 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const R f = (q < 2 ? factor : -factor) / (a[q] * a[q]);
-      contrib[slot + q] = cmk(f * Vq[q].x, f * Vq[q].y);
+      acc_add(cacc + kq[q], cmk(f * Vq[q].x, f * Vq[q].y));
     }
     put(i, model, 0, resid, 0);
   };
@@ -632,15 +647,15 @@ __device__ void fg_chisq(FgCtx<R>& c, const GroupCtx& g, double (&chi)[4]) {
     }
     const R va = dvar[i], vb = two ? dvar[ib] : va;
     const R ya = dre[i], yb = two ? dre[ib] : ya;
-    ca(i, Va, va, ya);
-    if (two) ca(ib, Vb, vb, yb);
+    ca(i, ka, Va, va, ya);
+    if (two) ca(ib, kb, Vb, vb, yb);
   }
   for (int q = 0; q < 4; ++q) chi[q] += acc[q].value();
 }
 
 // ---------------------------------------------------------------------------
-// F5: gather the derivative slots of each uv point (CSR) and spread
-// c_j = Vresre_j - i Vresim_j onto bandC.
+// F5: spread c_j = Vresre_j - i Vresim_j, read from the uv points'
+// derivative accumulators in the bin-sorted point order, onto bandC.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void atomic_add_r(double* p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add_r(float* p, float v) { atomicAdd(p, v); }
@@ -689,37 +704,12 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-// Sum of the chi-square derivative contributions of one uv point: its
-// entries ent[e0..e1) in the contribution slots, added in entry order.  Four
-// entries are fetched per step so their two dependent loads overlap.
-template <typename R>
-__device__ __forceinline__ void gather_contrib(const int* __restrict__ ent, const cpx<R>* __restrict__ contrib,
-                                               int e0, int e1, R& cre, R& cim) {
-  for (int e = e0; e < e1; e += 4) {
-    int k[4];
-    cpx<R> q[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) k[u] = e + u < e1 ? ent[e + u] : -1;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) q[u] = k[u] >= 0 ? contrib[k[u]] : cmk<R>(0, 0);
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (k[u] >= 0) {
-        cre += q[u].x;
-        cim += q[u].y;
-      }
-    }
-  }
-}
-
 __device__ void fg_spread_tc(FgCtx<float>& c, const GroupCtx& g) {
   const ProbDesc& P = *c.P;
   const float* xu = at<float>(c.base, P.o_u);
   const float* xv = at<float>(c.base, P.o_v);
-  const int* off = at<int>(c.base, P.o_csr_off);
-  const int* ent = at<int>(c.base, P.o_csr_ent);
   const int4* items = at<int4>(c.base, P.o_items);
-  const cpx<float>* contrib = at<cpx<float>>(c.base, P.o_contrib);
+  const cpx<float>* cacc = at<cpx<float>>(c.base, P.o_contrib);
   float* gband = at<float>(c.base, P.o_bandC);
   const int w = P.w;
   const int SG = 8 + w - 1;  // <= 16
@@ -750,8 +740,9 @@ __device__ void fg_spread_tc(FgCtx<float>& c, const GroupCtx& g) {
       int lr_l = 0, lc_l = 0;
       float* wr = wtab + lane * 2 * w;
       if (jl < item.y) {
-        gather_contrib(ent, contrib, off[jl], off[jl + 1], cre_l, cim_l);
-        cim_l = -cim_l;  // c = Vresre - i Vresim
+        const cpx<float> cj = cacc[jl];
+        cre_l = cj.x;
+        cim_l = -cj.y;  // c = Vresre - i Vresim
         const float xi1 = xu[jl], xi2 = xv[jl];
         const int l1 = (int)ceilf(xi1 - half), l2 = (int)ceilf(xi2 - half);
         for (int q = 0; q < w; ++q) {
@@ -844,10 +835,8 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
   const ProbDesc& P = *c.P;
   const R* xu = at<R>(c.base, P.o_u);
   const R* xv = at<R>(c.base, P.o_v);
-  const int* off = at<int>(c.base, P.o_csr_off);
-  const int* ent = at<int>(c.base, P.o_csr_ent);
   const int4* items = at<int4>(c.base, P.o_items);
-  const cpx<R>* contrib = at<cpx<R>>(c.base, P.o_contrib);
+  const cpx<R>* cacc = at<cpx<R>>(c.base, P.o_contrib);
   R* gband = at<R>(c.base, P.o_bandC);
   const int w = P.w, ww = P.w * P.w;
   const int SG = P.bin + w - 1;  // subgrid side
@@ -881,12 +870,14 @@ __device__ void fg_spread(FgCtx<R>& c, const GroupCtx& g) {
     const int4 item = items[it];
     for (int i = lane; i < SG * SG; i += 32) sub[i] = cmk<R>(0, 0);
     for (int jb = item.x; jb < item.y; jb += PB) {
-      // phase 1: lanes < PB prepare one point each (slots, cell, kernel weights)
+      // phase 1: lanes < PB prepare one point each (value, cell, kernel weights)
       const int jl = jb + lane;
       R cre_l = 0, cim_l = 0;
       int cell_l = 0;
       if (lane < PB && jl < item.y) {
-        gather_contrib(ent, contrib, off[jl], off[jl + 1], cre_l, cim_l);
+        const cpx<R> cj = cacc[jl];
+        cre_l = cj.x;
+        cim_l = cj.y;
         const R xi1 = xu[jl], xi2 = xv[jl];
         const int l1 = (int)ceil(xi1 - half), l2 = (int)ceil(xi2 - half);
         R* wr = wtab + lane * 2 * w;
@@ -1045,30 +1036,30 @@ struct PxGrid {
     return xg[(size_t)iy * nx + ix];
   }
 };
-template <class PX>
-__device__ __forceinline__ double tv_grade_px(const PX& px, int nx, int ny, int i1, int j1) {
+template <typename T, class PX>
+__device__ __forceinline__ T tv_grade_px(const PX& px, int nx, int ny, int i1, int j1) {
   // image.f90:512-612 with 0-based (i1, j1); reproduces the gradient reset
-  double gr = 0.0;
-  const double I11 = px(i1, j1);
-  double dIx = (i1 + 1 >= nx) ? 0.0 : px(i1 + 1, j1) - I11;
-  double dIy = (j1 + 1 >= ny) ? 0.0 : px(i1, j1 + 1) - I11;
-  double e = sqrt(dIx * dIx + dIy * dIy);
-  if (e > 1e-10) gr -= (dIx + dIy) / e;
+  T gr = 0;
+  const T I11 = (T)px(i1, j1);
+  T dIx = (i1 + 1 >= nx) ? (T)0 : (T)px(i1 + 1, j1) - I11;
+  T dIy = (j1 + 1 >= ny) ? (T)0 : (T)px(i1, j1 + 1) - I11;
+  T e = sqrt(dIx * dIx + dIy * dIy);
+  if (e > (T)1e-10) gr -= (dIx + dIy) / e;
   if (i1 - 1 >= 0) {
-    const double I01 = px(i1 - 1, j1);
+    const T I01 = (T)px(i1 - 1, j1);
     dIx = I11 - I01;
-    dIy = (j1 + 1 >= ny) ? 0.0 : px(i1 - 1, j1 + 1) - I01;
+    dIy = (j1 + 1 >= ny) ? (T)0 : (T)px(i1 - 1, j1 + 1) - I01;
     e = sqrt(dIx * dIx + dIy * dIy);
-    if (e > 1e-10) gr += dIx / e;
-    else gr = 0.0;
+    if (e > (T)1e-10) gr += dIx / e;
+    else gr = 0;
   }
   if (j1 - 1 >= 0) {
-    const double I10 = px(i1, j1 - 1);
+    const T I10 = (T)px(i1, j1 - 1);
     dIy = I11 - I10;
-    dIx = (i1 + 1 >= nx) ? 0.0 : px(i1 + 1, j1 - 1) - I10;
+    dIx = (i1 + 1 >= nx) ? (T)0 : (T)px(i1 + 1, j1 - 1) - I10;
     e = sqrt(dIx * dIx + dIy * dIy);
-    if (e > 1e-10) gr += dIy / e;
-    else gr = 0.0;
+    if (e > (T)1e-10) gr += dIy / e;
+    else gr = 0;
   }
   return gr;
 }
@@ -1118,7 +1109,16 @@ __device__ void frame_moments(const ProbDesc& P, char* base, double (&mom)[10]) 
   }
 }
 
-template <class PX>
+// log in the compute type of the regularizer stage
+__device__ __forceinline__ double reg_log(double x) { return log(x); }
+__device__ __forceinline__ float reg_log(float x) { return logf(x); }
+
+// Per-pixel regularizer terms in the compute type T (float in the FP32 mode):
+// L1, TV, TSV, MEM (kl) and the Gaussian-prior entropy (gs).  The moment
+// terms (total flux, centroid, second moment) use differences of image-wide
+// sums and stay in FP64; so do the regularizer sums, the gradient that the
+// optimiser reads and g.d.
+template <typename T, class PX>
 __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const RegMoments& rm, int lo, int hi,
                               double (&reg)[8], double& gd, double& sbg, bool opt_terms) {
   const double* x = at<double>(base, P.o_x);
@@ -1133,14 +1133,18 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
   const double* klw = P.has_kl ? at<double>(base, P.o_klw) : nullptr;
   const double* gsw = P.has_gs ? at<double>(base, P.o_gsw) : nullptr;
   const int nx = P.nx, ny = P.ny;
+  const T l1_l = (T)P.l1_l, tv_l = (T)P.tv_l, tsv_l = (T)P.tsv_l, kl_l = (T)P.kl_l, gs_l = (T)P.gs_l;
+  const double g_tfd = P.has_tfd ? P.tfd_l * 2 * rm.tfd_resid : 0.0;
   // running sums in registers (the caller's accumulators are written once
   // at the end, so the stores of the loop cannot alias them)
   double r0 = reg[0], r1 = reg[1], r2 = reg[2], r3 = reg[3], r4 = reg[4], gdl = gd, sbgl = sbg;
   for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
     const int ix = xi[p], iy = yi[p];
     const double I = x[p];
-    double gr = 0.0;
-    if (P.has_tfd) gr += P.tfd_l * 2 * rm.tfd_resid;
+    const T It = (T)I;
+    // each term is added to one FP64 sum, in the order of image.f90's
+    // gradient: total flux, centroid, l1, MEM, gs, TV, TSV, second moment
+    double gr = g_tfd;
     if (P.has_cen) {
       const double dix = (ix + 1) - P.nxref, diy = (iy + 1) - P.nyref;
       const double gIp = fabs(P.cen_alpha - 1) < 1e-10
@@ -1150,35 +1154,37 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
                        rm.cen_cost * gIp);
     }
     if (P.has_l1) {
-      const double a = smabs(I);
-      r0 += P.l1_l * l1w[p] * a;
-      gr += P.l1_l * l1w[p] * (I / a);
+      const T a = smabs(It), w = l1_l * (T)l1w[p];
+      r0 += (double)(w * a);
+      gr += (double)(w * (It / a));
     }
     if (P.has_kl) {
-      const double a = smabs(I), pr = klw[p];
-      r3 += P.kl_l * (a * log(a / pr) + pr / 2.718281828459045235);
-      gr += P.kl_l * (I / a) * (log(a / pr) + 1);
+      const T a = smabs(It), pr = (T)klw[p], lr = reg_log(a / pr);
+      r3 += (double)(kl_l * (a * lr + pr / (T)2.718281828459045235));
+      gr += (double)(kl_l * (It / a) * (lr + 1));
     }
     if (P.has_gs) {
-      const double a = smabs(I), pr = gsw[p];
-      r4 += P.gs_l * (a * (log(a / pr) - 1) + pr);
-      gr += P.gs_l * (I / a) * log(a / pr);
+      const T a = smabs(It), pr = (T)gsw[p], lr = reg_log(a / pr);
+      r4 += (double)(gs_l * (a * (lr - 1) + pr));
+      gr += (double)(gs_l * (It / a) * lr);
     }
     if (P.has_tv || P.has_tsv) {
-      const double dIx = (ix + 1 >= nx) ? 0.0 : px(ix + 1, iy) - I;
-      const double dIy = (iy + 1 >= ny) ? 0.0 : px(ix, iy + 1) - I;
+      const T dIx = (ix + 1 >= nx) ? (T)0 : (T)px(ix + 1, iy) - It;
+      const T dIy = (iy + 1 >= ny) ? (T)0 : (T)px(ix, iy + 1) - It;
       if (P.has_tv) {
-        r1 += P.tv_l * tvw[p] * sqrt(dIx * dIx + dIy * dIy);
-        gr += P.tv_l * tvw[p] * tv_grade_px(px, nx, ny, ix, iy);
+        const T w = tv_l * (T)tvw[p];
+        r1 += (double)(w * sqrt(dIx * dIx + dIy * dIy));
+        gr += (double)(w * tv_grade_px<T>(px, nx, ny, ix, iy));
       }
       if (P.has_tsv) {
-        r2 += P.tsv_l * tsvw[p] * (dIx * dIx + dIy * dIy);
-        double gt = 0.0;
-        if (ix + 1 < nx) gt -= 2 * (px(ix + 1, iy) - I);
-        if (iy + 1 < ny) gt -= 2 * (px(ix, iy + 1) - I);
-        if (ix - 1 >= 0) gt += 2 * (I - px(ix - 1, iy));
-        if (iy - 1 >= 0) gt += 2 * (I - px(ix, iy - 1));
-        gr += P.tsv_l * tsvw[p] * gt;
+        const T w = tsv_l * (T)tsvw[p];
+        r2 += (double)(w * (dIx * dIx + dIy * dIy));
+        T gt = 0;
+        if (ix + 1 < nx) gt -= 2 * ((T)px(ix + 1, iy) - It);
+        if (iy + 1 < ny) gt -= 2 * ((T)px(ix, iy + 1) - It);
+        if (ix - 1 >= 0) gt += 2 * (It - (T)px(ix - 1, iy));
+        if (iy - 1 >= 0) gt += 2 * (It - (T)px(ix, iy - 1));
+        gr += (double)(w * gt);
       }
     }
     if (P.has_sm) {
@@ -1212,14 +1218,15 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
 // F8: regularizer values and the full gradient g = grad chi2 + grad reg over
 // pixels [lo, hi); neighbours come from the dense image grid when F1 wrote
 // it in this evaluation (frames without data use the pixel map).
+template <typename T>
 __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, const RegMoments& rm,
                             int lo, int hi, double (&reg)[8], double& gd, double& sbg,
                             bool opt_terms = true) {
   if (P.nuv > 0 && P.o_xg) {
     const PxGrid px{at<double>(base, P.o_xg), P.nx, P.ny};
-    reg_grad_loop(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
+    reg_grad_loop<T>(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
   } else {
     const PxMap px{at<double>(base, P.o_x), at<int>(base, P.o_inv), P.nx, P.ny};
-    reg_grad_loop(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
+    reg_grad_loop<T>(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
   }
 }

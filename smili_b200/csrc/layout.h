@@ -35,7 +35,7 @@ struct ProbDesc {
   int w;                   // ES kernel width
   int b1s, b1n, b2s, b2n;  // band of fine-grid cells touched by the uv points
   int nfcv, namp, ncp, nca;
-  int nslot;               // contribution slots: nfcv + namp + 3 ncp + 4 nca
+  int nslot;               // uv references of the data (slots): nfcv + namp + 3 ncp + 4 nca
   int ndata;               // nfcv + namp + ncp + nca
   int nonneg, m, niter, prec64;
   int has_l1, has_tv, has_tsv, has_kl, has_gs, has_tfd, has_cen, has_sm;
@@ -68,9 +68,9 @@ struct ProbDesc {
   int64_t o_dre, o_dim, o_dvar;         // per datum: value(s) and variance (R)
   int64_t o_didx;                       // per slot: 0-based uv index (sorted order)
   int64_t o_dsgn;                       // per slot: sign (+1 / -1) as int8
-  int64_t o_csr_off, o_csr_ent;         // uv point -> contribution slots
   int64_t o_items;                      // int4 work items: start, end, row0, col0
-  int64_t o_tmpA, o_bandA, o_V, o_contrib, o_bandC, o_tmpC, o_gchi;
+  int64_t o_tmpA, o_bandA, o_V, o_contrib, o_bandC, o_tmpC, o_gchi;  // o_contrib: per uv point, the
+                                                                      // sum of the chi-square derivatives
   int64_t o_part;                       // FG partial sums [npart_ctas][SMILI_NPART] (double)
   // optimiser (double precision)
   int64_t o_x, o_g, o_z, o_r, o_d, o_t, o_xp, o_ws, o_wy, o_iwh, o_free, o_bkey;
@@ -87,7 +87,7 @@ struct ProbDesc {
 #define SMILI_PROB_OFFSETS(X)                                                                          \
   X(o_x0) X(o_xidx) X(o_yidx) X(o_inv) X(o_xg) X(o_ex) X(o_ey) X(o_l1w) X(o_tvw) X(o_tsvw) X(o_klw)  \
   X(o_gsw) X(o_dc1) X(o_dc2) X(o_tw1) X(o_tw2) X(o_u) X(o_v) X(o_dre) X(o_dim) X(o_dvar) X(o_didx)   \
-  X(o_dsgn) X(o_csr_off) X(o_csr_ent) X(o_items) X(o_tmpA) X(o_bandA) X(o_V) X(o_contrib) X(o_bandC) \
+  X(o_dsgn) X(o_items) X(o_tmpA) X(o_bandA) X(o_V) X(o_contrib) X(o_bandC) \
   X(o_tmpC) X(o_gchi) X(o_part) X(o_x) X(o_g) X(o_z) X(o_r) X(o_d) X(o_t) X(o_xp) X(o_ws) X(o_wy)     \
   X(o_iwh) X(o_free) X(o_bkey) X(o_sbk) X(o_sbi) X(o_hist) X(o_cand) X(o_lred) X(o_state) X(o_trace) \
   X(o_model) X(o_frames) X(o_rtw) X(o_riw) X(o_lcf) X(o_iavg) X(o_out)

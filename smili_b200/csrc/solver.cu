@@ -86,7 +86,7 @@ __device__ bool fg_stages(FgCtx<R>& fc, GroupCtx& g, int lo, int hi, double* red
     fg_t2_cols(fc, g);
     if (!group_sync(g)) return false;
     pf.mark(PR_F2);
-    fg_interp(fc, g);
+    fg_interp(fc, g, mode != MODE_T1);
     if (!group_sync(g)) return false;
     pf.mark(PR_F3);
     if (mode == MODE_T2) return true;
@@ -118,7 +118,7 @@ __device__ bool fg_stages(FgCtx<R>& fc, GroupCtx& g, int lo, int hi, double* red
     __syncthreads();
   }
   double reg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  fg_reg_grad(P, fc.base, g, rm, lo, hi, reg, acc[12], acc[13], opt_terms);
+  fg_reg_grad<R>(P, fc.base, g, rm, lo, hi, reg, acc[12], acc[13], opt_terms);
   for (int k = 0; k < 4; ++k) acc[k] += chi[k];
   for (int k = 0; k < 8; ++k) acc[4 + k] += reg[k];
   return true;
@@ -853,24 +853,17 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
       dvar[e] = (R)a.varca[i];
     }
   }
-  // uv point -> contribution slots (CSR); for the bare type-1 mode the slots
-  // are the uv points themselves with contrib = (Re c, -Im c)
-  std::vector<int> csr_off(nuv + 1, 0), csr_ent(std::max(nslot, 1));
+  // per-uv-point derivative accumulators: set here only for the bare type-1
+  // mode (c = (Re c, -Im c) in sorted order); otherwise F3 zeroes them and F4
+  // adds into them every evaluation
   std::vector<cpx<R>> contrib0;
   if (kind == PK_T1) {
-    for (int j = 0; j <= nuv; ++j) csr_off[j] = j;
     contrib0.resize(nuv);
     for (int j = 0; j < nuv; ++j) {
       const int o = perm[j];
-      csr_ent[j] = j;
       contrib0[j].x = (R)c_re[o];
       contrib0[j].y = (R)(-c_im[o]);
     }
-  } else {
-    for (int q = 0; q < nslot; ++q) csr_off[didx[q] + 1]++;
-    for (int j = 0; j < nuv; ++j) csr_off[j + 1] += csr_off[j];
-    std::vector<int> fillp(csr_off.begin(), csr_off.end() - 1);
-    for (int q = 0; q < nslot; ++q) csr_ent[fillp[didx[q]]++] = q;
   }
   // deconvolution factors and twiddles
   const std::vector<double> dc1 = deconv_factors(nx, d.nf1, w, beta), dc2 = deconv_factors(ny, d.nf2, w, beta);
@@ -909,13 +902,11 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.o_dvar = ar.take(sizeof(R) * dvar.size());
   d.o_didx = ar.take(sizeof(int) * didx.size());
   d.o_dsgn = ar.take(dsgn.size());
-  d.o_csr_off = ar.take(sizeof(int) * (nuv + 1));
-  d.o_csr_ent = ar.take(sizeof(int) * csr_ent.size());
   d.o_items = ar.take(sizeof(int) * items.size());
   d.o_tmpA = ar.take(C * (size_t)ny * d.b1n);
   d.o_bandA = ar.take(C * (size_t)d.b2n * d.b1n);
   d.o_V = ar.take(C * nuv);
-  d.o_contrib = ar.take(C * std::max(nslot, 1));
+  d.o_contrib = ar.take(C * std::max(nuv, 1));
   d.o_bandC = ar.take(C * (size_t)d.b2n * d.b1n);
   d.o_tmpC = ar.take(C * (size_t)d.b2n * nx);
   d.o_gchi = ar.take(sizeof(double) * (size_t)nx * ny);
@@ -982,8 +973,6 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   hp.put(d.o_dvar, dvar);
   hp.put(d.o_didx, didx);
   hp.put(d.o_dsgn, dsgn);
-  hp.put(d.o_csr_off, csr_off);
-  hp.put(d.o_csr_ent, csr_ent);
   hp.put(d.o_items, items);
   if (kind == PK_T1) hp.put(d.o_contrib, contrib0);
   // the original -> sorted uv permutation is needed to return visibilities

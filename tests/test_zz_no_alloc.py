@@ -66,8 +66,8 @@ def test_noalloc_honours_launch_options(problem, spread_bin, transform):
 def test_noalloc_rejects_oversize():
     from smili_b200 import _lib, synth
     from smili_b200.fortlib import fftim2d
-    # ~1e5 visibilities with closure terms: about 26 MB of FP64 arena
-    obs = synth.precision_path(seed=2, nx=64, nst=10, hours=12.0, scan_s=20.0, niter=1)
+    # 256x256 with ~1e5 visibilities and closure terms: about 24 MB of FP64 arena
+    obs = synth.precision_path(seed=2, nx=256, nst=10, hours=12.0, scan_s=20.0, niter=1)
     kw = make_kw(obs)
     with pytest.raises(_lib.SmiliError) as e:
         fftim2d.calc_cost_noalloc(kw["iin"], precision=64, **kw)
