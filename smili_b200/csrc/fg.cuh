@@ -1036,27 +1036,29 @@ struct PxGrid {
     return xg[(size_t)iy * nx + ix];
   }
 };
-template <typename T, class PX>
-__device__ __forceinline__ T tv_grade_px(const PX& px, int nx, int ny, int i1, int j1) {
-  // image.f90:512-612 with 0-based (i1, j1); reproduces the gradient reset
+// TV gradient (image.f90:512-612) at pixel (i1, j1) from preloaded values,
+// reproducing the gradient reset: I11 = I(i1, j1), xp = I(i1+1, j1),
+// yp = I(i1, j1+1), xm = I(i1-1, j1), ym = I(i1, j1-1), xmyp = I(i1-1, j1+1),
+// xpym = I(i1+1, j1-1); the has_* flags say which neighbours lie inside the
+// image (a value outside is never read).
+template <typename T>
+__device__ __forceinline__ T tv_grade_vals(T I11, T xp, T yp, T xm, T ym, T xmyp, T xpym, bool has_xp,
+                                           bool has_yp, bool has_xm, bool has_ym) {
   T gr = 0;
-  const T I11 = (T)px(i1, j1);
-  T dIx = (i1 + 1 >= nx) ? (T)0 : (T)px(i1 + 1, j1) - I11;
-  T dIy = (j1 + 1 >= ny) ? (T)0 : (T)px(i1, j1 + 1) - I11;
+  T dIx = has_xp ? xp - I11 : (T)0;
+  T dIy = has_yp ? yp - I11 : (T)0;
   T e = sqrt(dIx * dIx + dIy * dIy);
   if (e > (T)1e-10) gr -= (dIx + dIy) / e;
-  if (i1 - 1 >= 0) {
-    const T I01 = (T)px(i1 - 1, j1);
-    dIx = I11 - I01;
-    dIy = (j1 + 1 >= ny) ? (T)0 : (T)px(i1 - 1, j1 + 1) - I01;
+  if (has_xm) {
+    dIx = I11 - xm;
+    dIy = has_yp ? xmyp - xm : (T)0;
     e = sqrt(dIx * dIx + dIy * dIy);
     if (e > (T)1e-10) gr += dIx / e;
     else gr = 0;
   }
-  if (j1 - 1 >= 0) {
-    const T I10 = (T)px(i1, j1 - 1);
-    dIy = I11 - I10;
-    dIx = (i1 + 1 >= nx) ? (T)0 : (T)px(i1 + 1, j1 - 1) - I10;
+  if (has_ym) {
+    dIy = I11 - ym;
+    dIx = has_xp ? xpym - ym : (T)0;
     e = sqrt(dIx * dIx + dIy * dIy);
     if (e > (T)1e-10) gr += dIy / e;
     else gr = 0;
@@ -1138,9 +1140,29 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
   // running sums in registers (the caller's accumulators are written once
   // at the end, so the stores of the loop cannot alias them)
   double r0 = reg[0], r1 = reg[1], r2 = reg[2], r3 = reg[3], r4 = reg[4], gdl = gd, sbgl = sbg;
+  const bool nb = P.has_tv || P.has_tsv;
   for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
+    // every load of the iteration first (two dependent rounds: the pixel's
+    // indices, then its grid cell and neighbours), so that the arithmetic
+    // below waits once per round and not once per term
     const int ix = xi[p], iy = yi[p];
     const double I = x[p];
+    const double w_l1 = l1w ? l1w[p] : 0.0, w_kl = klw ? klw[p] : 0.0, w_gs = gsw ? gsw[p] : 0.0;
+    const double w_tv = tvw ? tvw[p] : 0.0, w_tsv = tsvw ? tsvw[p] : 0.0;
+    const double dp = opt_terms ? d[p] : 0.0;
+    const bool hxp = ix + 1 < nx, hyp = iy + 1 < ny, hxm = ix - 1 >= 0, hym = iy - 1 >= 0;
+    const double gc = gchi[(size_t)iy * nx + ix];
+    double vxp = 0, vyp = 0, vxm = 0, vym = 0, vxmyp = 0, vxpym = 0;
+    if (nb) {
+      vxp = hxp ? px(ix + 1, iy) : 0.0;
+      vyp = hyp ? px(ix, iy + 1) : 0.0;
+      vxm = hxm ? px(ix - 1, iy) : 0.0;
+      vym = hym ? px(ix, iy - 1) : 0.0;
+      if (P.has_tv) {
+        vxmyp = (hxm && hyp) ? px(ix - 1, iy + 1) : 0.0;
+        vxpym = (hxp && hym) ? px(ix + 1, iy - 1) : 0.0;
+      }
+    }
     const T It = (T)I;
     // each term is added to one FP64 sum, in the order of image.f90's
     // gradient: total flux, centroid, l1, MEM, gs, TV, TSV, second moment
@@ -1154,36 +1176,37 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
                        rm.cen_cost * gIp);
     }
     if (P.has_l1) {
-      const T a = smabs(It), w = l1_l * (T)l1w[p];
+      const T a = smabs(It), w = l1_l * (T)w_l1;
       r0 += (double)(w * a);
       gr += (double)(w * (It / a));
     }
     if (P.has_kl) {
-      const T a = smabs(It), pr = (T)klw[p], lr = reg_log(a / pr);
+      const T a = smabs(It), pr = (T)w_kl, lr = reg_log(a / pr);
       r3 += (double)(kl_l * (a * lr + pr / (T)2.718281828459045235));
       gr += (double)(kl_l * (It / a) * (lr + 1));
     }
     if (P.has_gs) {
-      const T a = smabs(It), pr = (T)gsw[p], lr = reg_log(a / pr);
+      const T a = smabs(It), pr = (T)w_gs, lr = reg_log(a / pr);
       r4 += (double)(gs_l * (a * (lr - 1) + pr));
       gr += (double)(gs_l * (It / a) * lr);
     }
-    if (P.has_tv || P.has_tsv) {
-      const T dIx = (ix + 1 >= nx) ? (T)0 : (T)px(ix + 1, iy) - It;
-      const T dIy = (iy + 1 >= ny) ? (T)0 : (T)px(ix, iy + 1) - It;
+    if (nb) {
+      const T txp = (T)vxp, typ = (T)vyp, txm = (T)vxm, tym = (T)vym;
+      const T dIx = hxp ? txp - It : (T)0;
+      const T dIy = hyp ? typ - It : (T)0;
       if (P.has_tv) {
-        const T w = tv_l * (T)tvw[p];
+        const T w = tv_l * (T)w_tv;
         r1 += (double)(w * sqrt(dIx * dIx + dIy * dIy));
-        gr += (double)(w * tv_grade_px<T>(px, nx, ny, ix, iy));
+        gr += (double)(w * tv_grade_vals<T>(It, txp, typ, txm, tym, (T)vxmyp, (T)vxpym, hxp, hyp, hxm, hym));
       }
       if (P.has_tsv) {
-        const T w = tsv_l * (T)tsvw[p];
+        const T w = tsv_l * (T)w_tsv;
         r2 += (double)(w * (dIx * dIx + dIy * dIy));
         T gt = 0;
-        if (ix + 1 < nx) gt -= 2 * ((T)px(ix + 1, iy) - It);
-        if (iy + 1 < ny) gt -= 2 * ((T)px(ix, iy + 1) - It);
-        if (ix - 1 >= 0) gt += 2 * (It - (T)px(ix - 1, iy));
-        if (iy - 1 >= 0) gt += 2 * (It - (T)px(ix, iy - 1));
+        if (hxp) gt -= 2 * (txp - It);
+        if (hyp) gt -= 2 * (typ - It);
+        if (hxm) gt += 2 * (It - txm);
+        if (hym) gt += 2 * (It - tym);
         gr += (double)(w * gt);
       }
     }
@@ -1197,10 +1220,10 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
       gr += P.sm_l * (2. * (rm.Sg[0] - rm.Sp[0]) * s0 + 2. * (rm.Sg[1] - rm.Sp[1]) * s1 +
                       4. * (rm.Sg[2] - rm.Sp[2]) * s2);
     }
-    const double gv = gchi[(size_t)iy * nx + ix] + gr;
+    const double gv = gc + gr;
     gout[p] = gv;
     if (!opt_terms) continue;  // a movie frame: the movie pass forms g.d and the projected gradient
-    gdl += gv * d[p];
+    gdl += gv * dp;
     // projected gradient (projgr, lbfgsb.f:2942-2990) with lower bound 0
     double gi = gv;
     if (P.nonneg && gi >= 0.0) gi = fmin(I, gi);

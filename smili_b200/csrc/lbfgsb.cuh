@@ -1169,8 +1169,15 @@ __device__ int lb_cmprlb_subsm(LbCtxT<SY>& c) {
   double ay[SMILI_MAXM_DEV], as[SMILI_MAXM_DEV];
 #pragma unroll
   for (int j = 0; j < SMILI_MAXM_DEV; ++j) ay[j] = as[j] = 0.0;
-  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
-    if (!unc && !c.freef[i]) continue;
+  // the free flag of the next element is fetched one iteration ahead, so
+  // the loads of an element wait for nothing but themselves
+  const int bd = blockDim.x;
+  int i = c.lo + threadIdx.x;
+  bool f_next = i < c.hi && (unc || c.freef[i]);
+  for (; i < c.hi; i += bd) {
+    const bool fr = f_next;
+    f_next = i + bd < c.hi && (unc || c.freef[i + bd]);
+    if (!fr) continue;
     // the row of W at pixel i, loaded once for r_i and for W'Z r
     double wyv[SMILI_MAXM_DEV], wsv[SMILI_MAXM_DEV];
 #pragma unroll
@@ -1232,16 +1239,28 @@ __device__ int lb_cmprlb_subsm(LbCtxT<SY>& c) {
     wr[j] = j < col ? wv_s[col + j] : 0.0;
   }
   const double rtheta = 1.0 / theta;
-  // one pass: d, the projected z and the directional derivative (z - x).g
-  for (int i = c.lo + threadIdx.x; i < c.hi; i += blockDim.x) {
-    const double zi = c.z[i];
+  // one pass: d, the projected z and the directional derivative (z - x).g;
+  // all loads of an element before its stores (which may alias them for the
+  // compiler), the free flag one element ahead
+  i = c.lo + threadIdx.x;
+  f_next = i < c.hi && (unc || c.freef[i]);
+  for (; i < c.hi; i += bd) {
+    const bool fr = f_next;
+    f_next = i + bd < c.hi && (unc || c.freef[i + bd]);
+    const double zi = c.z[i], xv = c.x[i], gvi = c.gv[i];
+    double ri = fr ? c.r[i] : 0.0;
+    SY wyr[SMILI_MAXM_DEV], wsr[SMILI_MAXM_DEV];
+#pragma unroll
+    for (int j = 0; j < SMILI_MAXM_DEV; ++j) {
+      wyr[j] = (fr && j < col) ? c.wy[(size_t)pj[j] * n + i] : (SY)0;
+      wsr[j] = (fr && j < col) ? c.ws[(size_t)pj[j] * n + i] : (SY)0;
+    }
     c.xp[i] = zi;
     double zn = zi;
-    if (c.freef[i] || unc) {
-      double ri = c.r[i];
+    if (fr) {
 #pragma unroll
       for (int j = 0; j < SMILI_MAXM_DEV; ++j)
-        if (j < col) ri += ld_wy(c, (size_t)pj[j] * n + i) * wq[j] / theta + ld_ws(c, (size_t)pj[j] * n + i) * wr[j];
+        if (j < col) ri += (double)wyr[j] * wq[j] / theta + (double)wsr[j] * wr[j];
       ri *= rtheta;
       c.r[i] = ri;
       if (P.nonneg) {
@@ -1252,7 +1271,7 @@ __device__ int lb_cmprlb_subsm(LbCtxT<SY>& c) {
       }
       c.z[i] = zn;
     }
-    acc2[1] += (zn - c.x[i]) * c.gv[i];
+    acc2[1] += (zn - xv) * gvi;
   }
   if (threadIdx.x == 0) {
     c.ops[0] = RED_MAX;
