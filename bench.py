@@ -286,15 +286,16 @@ class WarmStart:
     One step: K FP32 iterations of every problem from its prior, the U-Net's
     proposal from each K-iteration image, then the remaining niter - K FP32
     iterations from the proposals, with the same targets as the cold arm.
-    Both phases are launches of one device-resident batch: between them
-    ``Batch.set_niter`` changes the iteration caps and ``Batch.set_start``
-    replaces the start images (the priors are put back at the start of the
-    next step).  A problem that reaches its target in the first K
-    iterations counts there and restarts from its own image.  The step's
-    time is the two launches' CUDA event times, the network's forward pass
-    (CUDA events) and the host work around them (restoring the priors,
-    fetching the K-iteration images, forming the network input, turning its
-    output into starting vectors and uploading them; wall clock)."""
+    Both phases are launches of one device-resident batch, and the images
+    never leave the device: between the launches ``Batch.images`` writes the
+    K-iteration images as the network's input grid, the network runs on it,
+    and ``Batch.set_starts_from_images`` turns its output into every
+    problem's start image (``Batch.set_niter`` changes the iteration caps;
+    ``Batch.reset_starts`` puts the priors back at the start of the next
+    step).  A problem that reaches its target in the first K iterations
+    counts there and restarts from its own image.  The step's time is the
+    two launches' CUDA event times, the network's forward pass (CUDA events)
+    and the calls around them (wall clock)."""
 
     def __init__(self, probs, kws, seed_of, ftarget, niter, G, device=0):
         import torch
@@ -305,44 +306,41 @@ class WarmStart:
         self.net = UNet.load(WARM_WEIGHTS, device=f"cuda:{device}")
         self.K, self.niter = closure.K_DEFAULT, niter
         self.kws, self.seed_of, self.B = kws, seed_of, len(probs)
-        self.prior = [np.asarray(kws[s]["iin"], dtype=np.float64) for s in seed_of]
         self.b = _lib.Batch(probs, niter=niter, options=_lib.make_options(32, 1e-6, G, device))
         self.b.set_targets(ftarget)
         nx = int(kws[0]["nx"])
-        self.net.predict(np.zeros((self.B, nx, nx), np.float32), batch=self.B)  # buffers and first-call set-up
+        self.img = torch.zeros((self.B, nx, nx), dtype=torch.float32, device=f"cuda:{device}")
+        self.net.forward(self.img)  # buffers and first-call set-up
+        torch.cuda.synchronize()
 
     def step(self):
-        from smili_b200.warmstart import data
-        torch, _lib, closure, B, b = self.torch, self.lib, self.closure, self.B, self.b
+        torch, _lib, B, b = self.torch, self.lib, self.B, self.b
         t0 = time.perf_counter()
         b.set_niter(self.K)
-        for p in range(B):
-            b.set_start(p, self.prior[p])
+        b.reset_starts()
         t_host = time.perf_counter() - t0
         ms_k = b.run()
         t0 = time.perf_counter()
-        early = [b.fetch(p) for p in range(B)]
-        imgs = closure.normalise([data.to_grid(self.kws[self.seed_of[p]], early[p][0]) for p in range(B)])
+        early = [b.info(p) for p in range(B)]
+        hit_k = np.array([e["task"] == _lib.TASK_TARGET for e in early])
+        b.images(self.img)
         t_host += time.perf_counter() - t0
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        pred = self.net.predict(imgs, batch=B)
+        pred = self.net.forward(self.img)[:, :, :, 0].float()
         e1.record()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hit_k = np.array([e[3]["task"] == _lib.TASK_TARGET for e in early])
-        for p in range(B):
-            x0 = early[p][0] if hit_k[p] else closure.warm_init(self.kws[self.seed_of[p]], pred[p], early[p][0])
-            b.set_start(p, x0)
+        b.set_starts_from_images(pred, keep=hit_k)
         b.set_niter(self.niter - self.K)
         t_host += time.perf_counter() - t0
         ms_w = b.run()
-        infos = [b.fetch(p)[3] for p in range(B)]
+        infos = [b.info(p) for p in range(B)]
         hit = hit_k | np.array([i["task"] == _lib.TASK_TARGET for i in infos])
         ms_net = e0.elapsed_time(e1)
         return {"s": (ms_k + ms_net + ms_w) / 1000.0 + t_host, "hits": int(hit.sum()),
                 "kernel_s": (ms_k + ms_w) / 1000.0,
-                "nfg": int(sum(e[3]["nfg"] for e in early) + sum(i["nfg"] for i in infos)),
+                "nfg": int(sum(e["nfg"] for e in early) + sum(i["nfg"] for i in infos)),
                 "iterations": int(sum(self.K if h else self.K + i["niter"] for h, i in zip(hit_k, infos))),
                 "parts_s": {"first_K_iterations_device": ms_k / 1000.0, "unet_forward_device": ms_net / 1000.0,
                             "host": t_host, "remaining_iterations_device": ms_w / 1000.0}}
@@ -356,6 +354,8 @@ class WarmStart:
 
 WARM_WEIGHTS = os.path.join(ROOT, "smili_b200", "warmstart", "unet_closure256.npz")
 WARM_K = 50  # FP32 iterations before the proposal (smili_b200.warmstart.closure.K_DEFAULT)
+WARM_HELPER_LAUNCHES = 2  # smili_batch_images and smili_batch_set_starts_from_images
+PROB_RESULT_BYTES = 20 * 8 + 4 * 4  # ProbResult: terms[SMILI_NTERMS3D] and four counters
 
 
 def survey_cfg3(nprob, niter, device=0, nplain=8):
@@ -801,17 +801,19 @@ def main():
         fp32["reached_target_per_step"] = step_hits
         fp32["parts_s"] = {k: float(np.mean([r["parts_s"][k] for r in steps])) for k in steps[0]["parts_s"]}
         ws.close()
-        launches = UNET_FORWARD_LAUNCHES + 2
+        launches = UNET_FORWARD_LAUNCHES + 2 + WARM_HELPER_LAUNCHES
         # end to end from host buffers: packing and upload of the problems,
-        # the step (start images uploaded twice inside), download
-        h2d = h2d_prob + 2 * 8 * npix_all
-        d2h = 2 * (2 * 8 * npix_all + 15 * 8 * B) + 8 * npix_all
+        # targets, iteration caps (twice) and keep flags; per-problem results
+        # read after each launch; the final images, gradients and terms
+        h2d = h2d_prob + B * (8 + 2 * 4 + 1)
+        d2h = sum(2 * 8 * p.npix for p in probs) + B * (15 * 8 + 2 * PROB_RESULT_BYTES)
     else:
         ms_step, kernel_s = cold["ms_per_step"], cold["ms_per_step"] / 1000.0
         step_hits, fp32 = cold_hits, cold
         nfg, iters = cold_nfg, cold_iters
         launches = 1
-        h2d, d2h = h2d_prob, sum(8 * p.npix + 15 * 8 for p in probs)
+        h2d = h2d_prob + B * 8
+        d2h = sum(2 * 8 * p.npix for p in probs) + B * (15 * 8 + PROB_RESULT_BYTES)
     reached = float(np.mean(step_hits))
 
     # end to end through the C ABI from host buffers

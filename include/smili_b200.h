@@ -134,6 +134,30 @@ int smili_batch_set_start(smili_batch* b, int p, const double* x);
  * those caps.  With smili_batch_set_start this lets one device-resident
  * batch run a few iterations, restart from new images and run the rest. */
 int smili_batch_set_niter(smili_batch* b, const int* niter);
+
+/* Device-side warm start (no reference counterpart), for a batch whose
+ * problems are all nx x ny 2D images.  The three calls run on the batch's
+ * stream and return once their work is done.
+ *
+ * smili_batch_images: every problem's current image (its pixel vector after
+ * the last run) as a dense grid scaled to max 1: dst[p][iy][ix] =
+ * x_p(ix, iy) / max x_p, zero at cells outside the problem's pixels (all
+ * zero where max x_p <= 0).  dst: device memory on the batch's device,
+ * nprob * ny * nx floats.
+ *
+ * smili_batch_set_starts_from_images: replaces every problem's start image.
+ * For problem p the start is relu(img[p]) at its pixels, scaled so that it
+ * sums to the total of its current image x_p; it is x_p itself where
+ * keep[p] != 0, where relu(img[p]) has a non-finite cell or no positive one,
+ * or where x_p sums to <= 0.  img: device memory, nprob * ny * nx floats,
+ * complete before the call; keep: host array of nprob bytes, or NULL.
+ *
+ * smili_batch_reset_starts: puts back the start images the problems were
+ * created with. */
+int smili_batch_images(smili_batch* b, float* dst, int nx, int ny);
+int smili_batch_set_starts_from_images(smili_batch* b, const float* img, int nx, int ny,
+                                       const unsigned char* keep);
+int smili_batch_reset_starts(smili_batch* b);
 /* Cost recorded at each completed iteration of problem p (NaN where absent). */
 int smili_batch_trace(smili_batch* b, int p, double* trace, int len);
 void smili_batch_destroy(smili_batch* b);

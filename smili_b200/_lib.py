@@ -105,7 +105,8 @@ EXPORTS = ["smili_fftim2d_imaging", "smili_calc_cost", "smili_batch_create", "sm
            "smili_batch_fetch", "smili_batch_trace", "smili_batch_destroy", "smili_nufft_fwd_real",
            "smili_nufft_adj_real1d", "smili_last_error", "smili_version", "smili_batch_profile",
            "smili_batch_set_targets", "smili_calc_cost_noalloc", "smili_fftim3d_imaging",
-           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist", "smili_batch_set_start", "smili_batch_set_niter"]
+           "smili_calc_cost3d", "smili_model_terms", "smili_get_uvlist", "smili_batch_set_start", "smili_batch_set_niter",
+           "smili_batch_images", "smili_batch_set_starts_from_images", "smili_batch_reset_starts"]
 STAGES = ["t2_rows", "t2_cols", "interp", "chisq", "spread", "t1_rows", "t1_cols", "reg_grad",
           "lb_post", "cauchy", "formk", "subsm", "lnsrch", "init", "other", "n_fg", "c_select",
           "c_gather", "c_sort", "c_scan", "c_rounds"]
@@ -140,6 +141,9 @@ def lib():
         L.smili_batch_set_targets.argtypes = [vp, dp]
         L.smili_batch_set_start.argtypes = [vp, C.c_int, dp]
         L.smili_batch_set_niter.argtypes = [vp, ip]
+        L.smili_batch_images.argtypes = [vp, vp, C.c_int, C.c_int]
+        L.smili_batch_set_starts_from_images.argtypes = [vp, vp, C.c_int, C.c_int, vp]
+        L.smili_batch_reset_starts.argtypes = [vp]
         L.smili_nufft_fwd_real.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp, vp, dp, dp]
         L.smili_nufft_adj_real1d.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, vp, dp]
         _lib = L
@@ -304,6 +308,39 @@ class Batch:
         else:
             n = np.ascontiguousarray(np.broadcast_to(np.asarray(niter, dtype=np.int32), (self.n,)))
             check(lib().smili_batch_set_niter(self.h, n.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def info(self, p):
+        """Task, iteration and evaluation counts of problem p after the last run."""
+        info = SolveInfo()
+        check(lib().smili_batch_fetch(self.h, p, None, None, None, C.byref(info)))
+        return {"task": info.task, "niter": info.niter, "nfg": info.nfg, "error": info.error}
+
+    def images(self, dst):
+        """Every problem's current image, scaled to max 1, into the device
+        tensor dst of shape (n, ny, nx), float32 (all problems nx x ny)."""
+        n, ny, nx = dst.shape
+        if n != self.n or not dst.is_cuda or not dst.is_contiguous() or str(dst.dtype) != "torch.float32":
+            raise ValueError("dst must be a contiguous float32 CUDA tensor of shape (n, ny, nx)")
+        check(lib().smili_batch_images(self.h, C.c_void_p(dst.data_ptr()), int(nx), int(ny)))
+
+    def set_starts_from_images(self, img, keep=None):
+        """Start images from the device tensor img (n, ny, nx), float32: relu(img)
+        at each problem's pixels scaled to its current image's total; the
+        current image where keep[p] (or where that is not possible)."""
+        n, ny, nx = img.shape
+        if n != self.n or not img.is_cuda or not img.is_contiguous() or str(img.dtype) != "torch.float32":
+            raise ValueError("img must be a contiguous float32 CUDA tensor of shape (n, ny, nx)")
+        k = None
+        if keep is not None:
+            k = np.ascontiguousarray(np.asarray(keep, dtype=bool).astype(np.uint8))
+            if k.size != self.n:
+                raise ValueError("keep needs one flag per problem")
+        check(lib().smili_batch_set_starts_from_images(
+            self.h, C.c_void_p(img.data_ptr()), int(nx), int(ny), None if k is None else k.ctypes.data_as(C.c_void_p)))
+
+    def reset_starts(self):
+        """Put back the start images the problems were created with."""
+        check(lib().smili_batch_reset_starts(self.h))
 
     def set_start(self, p, x):
         """Problem p starts its next run from the pixel vector x (scaled units)."""

@@ -1005,6 +1005,10 @@ struct smili_batch {
   size_t dyn_bytes = 0;
   int profile = 0;
   std::vector<int> niter_cap;  // iteration caps at packing (trace buffers are sized for them)
+  // start images as packed, saved before the first replacement (reset_starts)
+  double* d_x0_saved = nullptr;
+  std::vector<size_t> x0_saved_off;
+  unsigned char* d_keep = nullptr;  // keep flags of set_starts_from_images
 };
 
 namespace {
@@ -1667,6 +1671,111 @@ int smili_batch_set_niter(smili_batch* b, const int* niter) {
   });
 }
 
+namespace {
+
+// Saves every problem's packed start image once, before the first call that
+// replaces one (reset_starts puts them back).
+int save_starts(smili_batch* b) {
+  if (b->d_x0_saved) return SMILI_OK;
+  size_t total = 0;
+  b->x0_saved_off.assign(b->nprob, 0);
+  for (int p = 0; p < b->nprob; ++p) {
+    b->x0_saved_off[p] = total;
+    if (b->descs[p].o_x0 && b->descs[p].nframes == 0) total += (size_t)b->descs[p].npix;
+  }
+  CUDA_TRY(cudaMalloc(&b->d_x0_saved, sizeof(double) * std::max<size_t>(total, 1)));
+  for (int p = 0; p < b->nprob; ++p) {
+    const ProbDesc& d = b->descs[p];
+    if (!d.o_x0 || d.nframes > 0) continue;
+    CUDA_TRY(cudaMemcpyAsync(b->d_x0_saved + b->x0_saved_off[p], b->d_arena + d.o_x0, sizeof(double) * d.npix,
+                             cudaMemcpyDeviceToDevice, b->stream));
+  }
+  return SMILI_OK;
+}
+
+// checks shared by the device-side warm-start calls
+int check_images(smili_batch* b, int nx, int ny) {
+  if (nx <= 0 || ny <= 0) return fail(SMILI_ERR_ARG, "invalid grid size");
+  for (const ProbDesc& d : b->descs)
+    if (!d.o_x0 || d.nframes > 0 || d.nx != nx || d.ny != ny)
+      return fail(SMILI_ERR_UNSUPPORTED, "every problem must be an nx x ny 2D image with a replaceable start");
+  return SMILI_OK;
+}
+
+constexpr int kWarmThreads = 256;
+
+__device__ double block_sum(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__device__ double block_max(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + st]);
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// one block per problem: its current image as a dense grid scaled to max 1
+__global__ void __launch_bounds__(kWarmThreads) batch_images_kernel(const ProbDesc* descs, const char* arena,
+                                                                    float* dst, int nx, int ny) {
+  __shared__ double sh[kWarmThreads];
+  const ProbDesc& d = descs[blockIdx.x];
+  const double* x = reinterpret_cast<const double*>(arena + d.o_x);
+  const int* xi = reinterpret_cast<const int*>(arena + d.o_xidx);
+  const int* yi = reinterpret_cast<const int*>(arena + d.o_yidx);
+  float* out = dst + (size_t)blockIdx.x * nx * ny;
+  double m = -INFINITY;
+  for (int i = threadIdx.x; i < d.npix; i += blockDim.x) m = fmax(m, x[i]);
+  m = block_max(m, sh);
+  for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) out[c] = 0.f;
+  __syncthreads();
+  if (m > 0.0)
+    for (int i = threadIdx.x; i < d.npix; i += blockDim.x) out[(size_t)yi[i] * nx + xi[i]] = (float)(x[i] / m);
+}
+
+// one block per problem: start image from relu(img), scaled to the current
+// image's total, or the current image itself
+__global__ void __launch_bounds__(kWarmThreads) batch_starts_kernel(const ProbDesc* descs, char* arena,
+                                                                    const float* img, int nx, int ny,
+                                                                    const unsigned char* keep) {
+  __shared__ double sh[kWarmThreads];
+  const ProbDesc& d = descs[blockIdx.x];
+  const double* x = reinterpret_cast<const double*>(arena + d.o_x);
+  const int* xi = reinterpret_cast<const int*>(arena + d.o_xidx);
+  const int* yi = reinterpret_cast<const int*>(arena + d.o_yidx);
+  double* x0 = reinterpret_cast<double*>(arena + d.o_x0);
+  const float* g = img + (size_t)blockIdx.x * nx * ny;
+  double s = 0.0, bad = 0.0, f = 0.0;
+  for (int c = threadIdx.x; c < nx * ny; c += blockDim.x) {
+    const float v = g[c];
+    if (!isfinite(v)) bad = 1.0;
+    else if (v > 0.f) s += (double)v;
+  }
+  for (int i = threadIdx.x; i < d.npix; i += blockDim.x) f += x[i];
+  s = block_sum(s, sh);
+  f = block_sum(f, sh);
+  bad = block_max(bad, sh);
+  const bool own = (keep && keep[blockIdx.x]) || bad > 0.0 || !(s > 0.0) || !(f > 0.0);
+  const double sc = own ? 0.0 : f / s;
+  for (int i = threadIdx.x; i < d.npix; i += blockDim.x)
+    x0[i] = own ? x[i] : (double)fmaxf(g[(size_t)yi[i] * nx + xi[i]], 0.f) * sc;
+}
+
+}  // namespace
+
 int smili_batch_set_start(smili_batch* b, int p, const double* x) {
   return guarded([&]() -> int {
     if (!b || p < 0 || p >= b->nprob || !x) return fail(SMILI_ERR_ARG, "invalid start-image request");
@@ -1675,7 +1784,58 @@ int smili_batch_set_start(smili_batch* b, int p, const double* x) {
     for (int i = 0; i < d.npix; ++i)
       if (!std::isfinite(x[i])) return fail(SMILI_ERR_DATA, "non-finite start image");
     CUDA_TRY(cudaSetDevice(b->device));
+    const int rc = save_starts(b);
+    if (rc != SMILI_OK) return rc;
     CUDA_TRY(cudaMemcpyAsync(b->d_arena + d.o_x0, x, sizeof(double) * d.npix, cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return SMILI_OK;
+  });
+}
+
+int smili_batch_images(smili_batch* b, float* dst, int nx, int ny) {
+  return guarded([&]() -> int {
+    if (!b || !dst) return fail(SMILI_ERR_ARG, "null argument");
+    int rc = check_images(b, nx, ny);
+    if (rc != SMILI_OK) return rc;
+    CUDA_TRY(cudaSetDevice(b->device));
+    batch_images_kernel<<<b->nprob, kWarmThreads, 0, b->stream>>>(b->d_descs, b->d_arena, dst, nx, ny);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return SMILI_OK;
+  });
+}
+
+int smili_batch_set_starts_from_images(smili_batch* b, const float* img, int nx, int ny,
+                                       const unsigned char* keep) {
+  return guarded([&]() -> int {
+    if (!b || !img) return fail(SMILI_ERR_ARG, "null argument");
+    int rc = check_images(b, nx, ny);
+    if (rc != SMILI_OK) return rc;
+    CUDA_TRY(cudaSetDevice(b->device));
+    if ((rc = save_starts(b)) != SMILI_OK) return rc;
+    if (keep) {
+      if (!b->d_keep) CUDA_TRY(cudaMalloc(&b->d_keep, b->nprob));
+      CUDA_TRY(cudaMemcpyAsync(b->d_keep, keep, b->nprob, cudaMemcpyHostToDevice, b->stream));
+    }
+    batch_starts_kernel<<<b->nprob, kWarmThreads, 0, b->stream>>>(b->d_descs, b->d_arena, img, nx, ny,
+                                                                  keep ? b->d_keep : nullptr);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return SMILI_OK;
+  });
+}
+
+int smili_batch_reset_starts(smili_batch* b) {
+  return guarded([&]() -> int {
+    if (!b) return fail(SMILI_ERR_ARG, "null batch");
+    if (!b->d_x0_saved) return SMILI_OK;  // nothing was replaced
+    CUDA_TRY(cudaSetDevice(b->device));
+    for (int p = 0; p < b->nprob; ++p) {
+      const ProbDesc& d = b->descs[p];
+      if (!d.o_x0 || d.nframes > 0) continue;
+      CUDA_TRY(cudaMemcpyAsync(b->d_arena + d.o_x0, b->d_x0_saved + b->x0_saved_off[p], sizeof(double) * d.npix,
+                               cudaMemcpyDeviceToDevice, b->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(b->stream));
     return SMILI_OK;
   });
@@ -1700,6 +1860,8 @@ void smili_batch_destroy(smili_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->d_arena) cudaFree(b->d_arena);
   if (b->d_aux) cudaFree(b->d_aux);
+  if (b->d_x0_saved) cudaFree(b->d_x0_saved);
+  if (b->d_keep) cudaFree(b->d_keep);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }

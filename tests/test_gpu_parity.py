@@ -300,6 +300,53 @@ def test_set_niter_equals_packing(crescent32, lib):
     b.close()
 
 
+def test_device_warm_start_matches_host(crescent32, lib):
+    """smili_batch_images, smili_batch_set_starts_from_images and
+    smili_batch_reset_starts do on the device what the host warm start does
+    with fetch, to_grid, normalise, warm_init and set_start."""
+    import torch
+    from smili_b200.warmstart import closure, data
+    kw = make_kw(crescent32, niter=8)
+    rng = np.random.default_rng(5)
+    kws = [dict(kw, iin=np.asarray(kw["iin"]) * rng.uniform(0.5, 1.5, np.size(kw["iin"]))) for _ in range(3)]
+    opts = lib.make_options(64, 1e-9)
+    b = lib.Batch(kws, niter=8, options=opts)
+    b.run()
+    xs = [b.fetch(p)[0] for p in range(3)]
+    nx, ny = int(kw["nx"]), int(kw["ny"])
+    img = torch.zeros((3, ny, nx), dtype=torch.float32, device="cuda")
+    b.images(img)
+    want = closure.normalise([data.to_grid(k, x) for k, x in zip(kws, xs)])
+    np.testing.assert_allclose(img.cpu().numpy(), want, rtol=1e-6, atol=1e-7)
+    pred = rng.standard_normal((3, ny, nx)).astype(np.float32)
+    pred[2] = -np.abs(pred[2])  # no positive cell: the current image is kept
+    keep = np.array([False, True, False])
+    b.set_starts_from_images(torch.as_tensor(pred, device="cuda"), keep=keep)
+    starts = [xs[p] if keep[p] else closure.warm_init(kws[p], pred[p], xs[p]) for p in range(3)]
+    b.run()
+    c = lib.Batch([dict(k, iin=s) for k, s in zip(kws, starts)], niter=8, options=opts)
+    c.run()
+    for p in range(3):
+        _, t, _, i = b.fetch(p)
+        _, t2, _, i2 = c.fetch(p)
+        assert i["niter"] == i2["niter"]
+        assert abs(t["cost"] - t2["cost"]) <= 1e-8 * abs(t2["cost"])
+    c.close()
+    b.reset_starts()
+    b.run()
+    d = lib.Batch(kws, niter=8, options=opts)
+    d.run()
+    for p in range(3):
+        _, t, _, i = b.fetch(p)
+        _, t2, _, i2 = d.fetch(p)
+        assert i["niter"] == i2["niter"]
+        assert abs(t["cost"] - t2["cost"]) <= 1e-8 * abs(t2["cost"])
+    d.close()
+    with pytest.raises(ValueError):
+        b.images(torch.zeros((2, ny, nx), dtype=torch.float32, device="cuda"))
+    b.close()
+
+
 def test_invalid_inputs_raise(crescent32, lib):
     kw = make_kw(crescent32, niter=5)
     bad = dict(kw)
