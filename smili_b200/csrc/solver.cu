@@ -853,6 +853,43 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
       dvar[e] = (R)a.varca[i];
     }
   }
+  // Order the data of each type by the sorted position of their first uv
+  // point (stable): neighbouring threads of the chi-square stage then gather
+  // neighbouring model visibilities and add into neighbouring accumulators,
+  // so an amplitude or visibility warp touches a few sectors instead of 32.
+  // The sums only change order.  Per-datum models (PK_MODEL) keep the
+  // callers' order.
+  if (kind != PK_MODEL && d.ndata > 1) {
+    auto reorder = [&](int e0, int ne, int s0, int nref) {
+      if (ne < 2) return;
+      std::vector<int> ord(ne);
+      std::iota(ord.begin(), ord.end(), 0);
+      std::stable_sort(ord.begin(), ord.end(),
+                       [&](int p, int q) { return didx[s0 + nref * p] < didx[s0 + nref * q]; });
+      std::vector<R> r0(ne), r1(ne), r2(ne);
+      std::vector<int> ix((size_t)ne * nref);
+      std::vector<signed char> sg((size_t)ne * nref);
+      for (int i = 0; i < ne; ++i) {
+        const int o = ord[i];
+        r0[i] = dre[e0 + o];
+        r1[i] = dim[e0 + o];
+        r2[i] = dvar[e0 + o];
+        for (int q = 0; q < nref; ++q) {
+          ix[(size_t)nref * i + q] = didx[s0 + nref * o + q];
+          sg[(size_t)nref * i + q] = dsgn[s0 + nref * o + q];
+        }
+      }
+      std::copy(r0.begin(), r0.end(), dre.begin() + e0);
+      std::copy(r1.begin(), r1.end(), dim.begin() + e0);
+      std::copy(r2.begin(), r2.end(), dvar.begin() + e0);
+      std::copy(ix.begin(), ix.end(), didx.begin() + s0);
+      std::copy(sg.begin(), sg.end(), dsgn.begin() + s0);
+    };
+    reorder(0, nfcv, 0, 1);
+    reorder(nfcv, namp, nfcv, 1);
+    reorder(nfcv + namp, ncp, nfcv + namp, 3);
+    reorder(nfcv + namp + ncp, nca, nfcv + namp + 3 * ncp, 4);
+  }
   // per-uv-point derivative accumulators: set here only for the bare type-1
   // mode (c = (Re c, -Im c) in sorted order); otherwise F3 zeroes them and F4
   // adds into them every evaluation
