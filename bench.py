@@ -546,7 +546,9 @@ def profile_case(case, device=0):
     - ``t2`` / ``t1``: one FP32 type-2 / type-1 transform of the workload's
       97 200 uv points on the 256 x 256 grid (the transform stages alone);
     - ``conv``: the U-Net convolution 32 x 64 x 64, 192 -> 192 channels,
-      timed with CUDA events on the tcgen05 path and the mma.sync path.
+      timed with CUDA events on the tcgen05 path and the mma.sync path;
+    - ``train``: U-Net training steps (forward, backward, Adam) on 32 images
+      of 128 x 128, timed with CUDA events.
 
     Inputs come from the library's own transform (fast), not the exact DFT."""
     from smili_b200 import _lib, synth
@@ -610,6 +612,34 @@ def profile_case(case, device=0):
             out[name] = {"ms": ms, "tflops": out["gflop"] / ms}
         K.set_conv_path(0)
         print(json.dumps(out))
+    elif case == "train":
+        import torch
+        from smili_b200.warmstart.train import unet_flops
+        from smili_b200.warmstart.unet import UNet
+        B, H = 32, 128
+        rng = np.random.default_rng(0)
+        X = rng.random((B, H, H), dtype=np.float32)
+        Y = rng.random((B, H, H), dtype=np.float32)
+        net = UNet(seed=0, device=f"cuda:{device}")
+        xt, yt = torch.as_tensor(X, device=net.device), torch.as_tensor(Y, device=net.device)
+
+        def step():
+            net.forward(xt)
+            net.loss(yt)
+            net.backward()
+            net.adam_step(1e-4)
+        for _ in range(5):
+            step()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 20
+        flops = 3 * unet_flops(net, H, H) * B  # forward, data gradient, weight gradient
+        print(json.dumps({"case": case, "batch": B, "image": H, "ms_per_step": ms,
+                          "tflops": flops / (ms / 1000.0) / 1e12, "nparam": int(net.nparam)}))
     else:
         raise SystemExit(f"unknown case {case}")
 
@@ -640,7 +670,7 @@ def main():
                     help="time the cold arm (prior starts) as the headline instead of the learned warm start")
     ap.add_argument("--warm-problems", type=int, default=256,
                     help="held-out problems of the learned warm-start comparison (0: skip)")
-    ap.add_argument("--case", default=None, choices=["traffic", "stages", "fg", "t2", "t1", "conv"],
+    ap.add_argument("--case", default=None, choices=["traffic", "stages", "fg", "t2", "t1", "conv", "train"],
                     help="run one small launch for a profiler capture instead of the benchmark")
     args = ap.parse_args()
     if args.case:
