@@ -134,9 +134,9 @@ __device__ void dft_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
         const int rr = i / DFT_KC, kk = i - rr * DFT_KC, iy = y0 + rr, ix = k0 + kk;
         R u = 0;
         if (iy < ny && ix < nx) {
-          const int pv = inv[iy * nx + ix];
+          const int pv = P.ident ? iy * nx + ix : inv[iy * nx + ix];
           const double val = pv >= 0 ? x[pv] : 0.0;
-          xg[(size_t)iy * nx + ix] = val;
+          if (!P.ident) xg[(size_t)iy * nx + ix] = val;
           u = (R)(val * dc1[ix] * dc2[iy]);
           if (need_mom && pv >= 0) {
             const double fx = ix + 1, fy = iy + 1;  // 1-based pixel numbers as the reference
@@ -327,9 +327,9 @@ __device__ void fg_t2_rows(FgCtx<R>& c, const GroupCtx& g, double (&mom)[10]) {
     __syncthreads();
     for (int i = threadIdx.x; i < rows * nx; i += blockDim.x) {
       const int s = i / nx, ix = i - s * nx, iy = row0 + s;
-      const int pv = inv[iy * nx + ix];
+      const int pv = P.ident ? iy * nx + ix : inv[iy * nx + ix];
       const double val = pv >= 0 ? x[pv] : 0.0;
-      xg[(size_t)iy * nx + ix] = val;
+      if (!P.ident) xg[(size_t)iy * nx + ix] = val;
       c.sbuf[s * n1 + wrapn(ix - nx / 2, n1)] = cmk<R>((R)(val * dc1[ix] * dc2[iy]), (R)0);
       if (need_mom && pv >= 0) {
         const double fx = ix + 1, fy = iy + 1;  // 1-based pixel numbers as the reference
@@ -1141,11 +1141,19 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
   // at the end, so the stores of the loop cannot alias them)
   double r0 = reg[0], r1 = reg[1], r2 = reg[2], r3 = reg[3], r4 = reg[4], gdl = gd, sbgl = sbg;
   const bool nb = P.has_tv || P.has_tsv;
+  const bool ident = P.ident;
   for (int p = lo + threadIdx.x; p < hi; p += blockDim.x) {
     // every load of the iteration first (two dependent rounds: the pixel's
     // indices, then its grid cell and neighbours), so that the arithmetic
     // below waits once per round and not once per term
-    const int ix = xi[p], iy = yi[p];
+    int ix, iy;
+    if (ident) {  // row-major full grid: no index loads, so one round of loads below
+      iy = p / nx;
+      ix = p - iy * nx;
+    } else {
+      ix = xi[p];
+      iy = yi[p];
+    }
     const double I = x[p];
     const double w_l1 = l1w ? l1w[p] : 0.0, w_kl = klw ? klw[p] : 0.0, w_gs = gsw ? gsw[p] : 0.0;
     const double w_tv = tvw ? tvw[p] : 0.0, w_tsv = tsvw ? tsvw[p] : 0.0;
@@ -1245,8 +1253,9 @@ template <typename T>
 __device__ void fg_reg_grad(const ProbDesc& P, char* base, const GroupCtx& g, const RegMoments& rm,
                             int lo, int hi, double (&reg)[8], double& gd, double& sbg,
                             bool opt_terms = true) {
-  if (P.nuv > 0 && P.o_xg) {
-    const PxGrid px{at<double>(base, P.o_xg), P.nx, P.ny};
+  if (P.ident || (P.nuv > 0 && P.o_xg)) {
+    // the dense grid: x itself on a row-major full grid, else the copy F1 wrote
+    const PxGrid px{at<double>(base, P.ident ? P.o_x : P.o_xg), P.nx, P.ny};
     reg_grad_loop<T>(P, base, px, rm, lo, hi, reg, gd, sbg, opt_terms);
   } else {
     const PxMap px{at<double>(base, P.o_x), at<int>(base, P.o_inv), P.nx, P.ny};

@@ -40,6 +40,8 @@ struct ProbDesc {
   int nonneg, m, niter, prec64;
   int has_l1, has_tv, has_tsv, has_kl, has_gs, has_tfd, has_cen, has_sm;
   int windowed;            // 1 when the pixel set is not the full nx*ny grid
+  int ident;               // 1 when pixel p is grid cell (p % nx, p / nx): the full grid in
+                           // row-major order, so x is its own dense image grid
   int nitems;              // spreading work items (<= 128 points of one bin x bin tile)
   int bin;                 // spreading bin side in fine-grid cells (8 or 16)
   int dft;                 // 1: the four band passes as dense products with the

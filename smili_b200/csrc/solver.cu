@@ -622,6 +622,8 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   d.nxref = a.nxref;
   d.nyref = a.nyref;
   d.windowed = N != nx * ny;
+  d.ident = !d.windowed;
+  for (int i = 0; d.ident && i < N; ++i) d.ident = xi[i] == i % nx && yi[i] == i / nx;
   // data terms
   const bool use_data = kind == PK_SOLVE || kind == PK_FG || kind == PK_MODEL || frame;
   const int nfcv = (use_data && a.isfcv) ? a.nfcv : 0;
