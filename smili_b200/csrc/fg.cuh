@@ -1129,11 +1129,13 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
   const double* gchi = at<double>(base, P.o_gchi);
   const double* d = at<double>(base, P.o_d);
   double* gout = at<double>(base, P.o_g);
-  const double* l1w = P.has_l1 ? at<double>(base, P.o_l1w) : nullptr;
-  const double* tvw = P.has_tv ? at<double>(base, P.o_tvw) : nullptr;
-  const double* tsvw = P.has_tsv ? at<double>(base, P.o_tsvw) : nullptr;
-  const double* klw = P.has_kl ? at<double>(base, P.o_klw) : nullptr;
-  const double* gsw = P.has_gs ? at<double>(base, P.o_gsw) : nullptr;
+  // a weight array is read only when its weights differ between pixels;
+  // otherwise its one value (wu) is used
+  const double* l1w = (P.has_l1 && !(P.wuni & 1)) ? at<double>(base, P.o_l1w) : nullptr;
+  const double* tvw = (P.has_tv && !(P.wuni & 2)) ? at<double>(base, P.o_tvw) : nullptr;
+  const double* tsvw = (P.has_tsv && !(P.wuni & 4)) ? at<double>(base, P.o_tsvw) : nullptr;
+  const double* klw = (P.has_kl && !(P.wuni & 8)) ? at<double>(base, P.o_klw) : nullptr;
+  const double* gsw = (P.has_gs && !(P.wuni & 16)) ? at<double>(base, P.o_gsw) : nullptr;
   const int nx = P.nx, ny = P.ny;
   const T l1_l = (T)P.l1_l, tv_l = (T)P.tv_l, tsv_l = (T)P.tsv_l, kl_l = (T)P.kl_l, gs_l = (T)P.gs_l;
   const double g_tfd = P.has_tfd ? P.tfd_l * 2 * rm.tfd_resid : 0.0;
@@ -1155,8 +1157,8 @@ __device__ void reg_grad_loop(const ProbDesc& P, char* base, const PX& px, const
       iy = yi[p];
     }
     const double I = x[p];
-    const double w_l1 = l1w ? l1w[p] : 0.0, w_kl = klw ? klw[p] : 0.0, w_gs = gsw ? gsw[p] : 0.0;
-    const double w_tv = tvw ? tvw[p] : 0.0, w_tsv = tsvw ? tsvw[p] : 0.0;
+    const double w_l1 = l1w ? l1w[p] : P.wu[0], w_kl = klw ? klw[p] : P.wu[3], w_gs = gsw ? gsw[p] : P.wu[4];
+    const double w_tv = tvw ? tvw[p] : P.wu[1], w_tsv = tsvw ? tsvw[p] : P.wu[2];
     const double dp = opt_terms ? d[p] : 0.0;
     const bool hxp = ix + 1 < nx, hyp = iy + 1 < ny, hxm = ix - 1 >= 0, hym = iy - 1 >= 0;
     const double gc = gchi[(size_t)iy * nx + ix];

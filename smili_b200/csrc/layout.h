@@ -55,6 +55,10 @@ struct ProbDesc {
   double beta;
   double wfcv, wamp, wcp, wca;       // normalised data weights (w / wtotal)
   double l1_l, tv_l, tsv_l, kl_l, gs_l, tfd_l, tfd_tgtfd, cen_l, cen_alpha;
+  // per-pixel regularizer weights that are one value over the whole image
+  // (flat priors): bit 0..4 of wuni for l1, tv, tsv, kl, gs, value in wu[]
+  int wuni;
+  double wu[5];
   double sm_l, sm_maj, sm_min, sm_phi;
   double nxref, nyref;
   double factr, pgtol;

@@ -572,6 +572,25 @@ struct HostProb {
 // PK_FRAME: one frame of a movie; PK_MODEL: one evaluation that also returns per-datum models
 enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4, PK_MODEL = 5 };
 
+// A regularizer whose per-pixel weights are one value (a flat prior) is
+// evaluated with that value instead of a load per pixel (the array is still
+// uploaded).
+void set_uniform_weights(ProbDesc& d, const smili_imaging_args& a, int N) {
+  const int has[5] = {d.has_l1, d.has_tv, d.has_tsv, d.has_kl, d.has_gs};
+  const double* w[5] = {a.l1_wgt, a.tv_wgt, a.tsv_wgt, a.kl_wgt, a.gs_wgt};
+  d.wuni = 0;
+  for (int k = 0; k < 5; ++k) {
+    d.wu[k] = 0.0;
+    if (!has[k] || !w[k] || N < 1) continue;
+    bool uni = true;
+    for (int i = 1; uni && i < N; ++i) uni = w[k][i] == w[k][0];
+    if (uni) {
+      d.wuni |= 1 << k;
+      d.wu[k] = w[k][0];
+    }
+  }
+}
+
 template <typename R>
 int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, int m, double factr,
                  double pgtol, double eps, Arena& ar, HostProb& hp, const double* x_override,
@@ -704,6 +723,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     if (d.has_tsv) hp.put(d.o_tsvw, std::vector<double>(a.tsv_wgt, a.tsv_wgt + N));
     if (d.has_kl) hp.put(d.o_klw, std::vector<double>(a.kl_wgt, a.kl_wgt + N));
     if (d.has_gs) hp.put(d.o_gsw, std::vector<double>(a.gs_wgt, a.gs_wgt + N));
+    set_uniform_weights(d, a, N);
     return SMILI_OK;
   }
 
@@ -984,6 +1004,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   if (d.has_tsv) hp.put(d.o_tsvw, std::vector<double>(a.tsv_wgt, a.tsv_wgt + N));
   if (d.has_kl) hp.put(d.o_klw, std::vector<double>(a.kl_wgt, a.kl_wgt + N));
   if (d.has_gs) hp.put(d.o_gsw, std::vector<double>(a.gs_wgt, a.gs_wgt + N));
+  set_uniform_weights(d, a, N);
   hp.put(d.o_dc1, dc1);
   hp.put(d.o_dc2, dc2);
   hp.put(d.o_tw1, twiddles(d.nf1));
