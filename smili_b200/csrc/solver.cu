@@ -561,16 +561,31 @@ bool finite_all(const double* p, int n) {
 struct HostProb {
   ProbDesc d;
   std::vector<std::pair<int64_t, std::vector<char>>> blobs;
+  // one copy of the bytes (no zero fill first)
+  template <typename T>
+  void put(int64_t off, const T* p, size_t n) {
+    const char* c = reinterpret_cast<const char*>(p);
+    blobs.emplace_back(off, std::vector<char>(c, c + n * sizeof(T)));
+  }
   template <typename T>
   void put(int64_t off, const std::vector<T>& v) {
-    std::vector<char> b(v.size() * sizeof(T));
-    if (!v.empty()) std::memcpy(b.data(), v.data(), b.size());
-    blobs.emplace_back(off, std::move(b));
+    put(off, v.data(), v.size());
   }
 };
 
 // PK_FRAME: one frame of a movie; PK_MODEL: one evaluation that also returns per-datum models
 enum { PK_SOLVE = 0, PK_FG = 1, PK_T2 = 2, PK_T1 = 3, PK_FRAME = 4, PK_MODEL = 5 };
+
+// The order of [0, n) by key(i) in [0, nkey), ties in index order: a
+// counting sort, the same order as std::stable_sort by key in O(n + nkey).
+template <class K>
+std::vector<int> counting_order(int n, int nkey, K key) {
+  std::vector<int> start((size_t)nkey + 1, 0), ord(n);
+  for (int i = 0; i < n; ++i) ++start[key(i) + 1];
+  for (int k = 0; k < nkey; ++k) start[k + 1] += start[k];
+  for (int i = 0; i < n; ++i) ord[start[key(i)]++] = i;
+  return ord;
+}
 
 // A regularizer whose per-pixel weights are one value (a flat prior) is
 // evaluated with that value instead of a load per pixel (the array is still
@@ -718,11 +733,11 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     hp.put(d.o_xidx, xi);
     hp.put(d.o_yidx, yi);
     hp.put(d.o_inv, inv);
-    if (d.has_l1) hp.put(d.o_l1w, std::vector<double>(a.l1_wgt, a.l1_wgt + N));
-    if (d.has_tv) hp.put(d.o_tvw, std::vector<double>(a.tv_wgt, a.tv_wgt + N));
-    if (d.has_tsv) hp.put(d.o_tsvw, std::vector<double>(a.tsv_wgt, a.tsv_wgt + N));
-    if (d.has_kl) hp.put(d.o_klw, std::vector<double>(a.kl_wgt, a.kl_wgt + N));
-    if (d.has_gs) hp.put(d.o_gsw, std::vector<double>(a.gs_wgt, a.gs_wgt + N));
+    if (d.has_l1) hp.put(d.o_l1w, a.l1_wgt, (size_t)N);
+    if (d.has_tv) hp.put(d.o_tvw, a.tv_wgt, (size_t)N);
+    if (d.has_tsv) hp.put(d.o_tsvw, a.tsv_wgt, (size_t)N);
+    if (d.has_kl) hp.put(d.o_klw, a.kl_wgt, (size_t)N);
+    if (d.has_gs) hp.put(d.o_gsw, a.gs_wgt, (size_t)N);
     set_uniform_weights(d, a, N);
     return SMILI_OK;
   }
@@ -783,15 +798,16 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     long r = a % n;
     return r < 0 ? r + n : r;
   };
-  std::vector<int> perm(nuv);
-  std::iota(perm.begin(), perm.end(), 0);
   std::vector<long> bkey(nuv);
+  std::vector<int> bidx(nuv);
+  const int nb1 = (d.nf1 + bin - 1) / bin, nb2 = (d.nf2 + bin - 1) / bin;
   for (int j = 0; j < nuv; ++j) {
     const long c1 = imodh((long)std::ceil(xu[j] - half) - d.b1s, d.nf1);
     const long c2 = imodh((long)std::ceil(xv[j] - half) - d.b2s, d.nf2);
     bkey[j] = ((c2 / bin) << 32) + (c1 / bin);
+    bidx[j] = (int)(c2 / bin) * nb1 + (int)(c1 / bin);  // the same order as bkey
   }
-  std::stable_sort(perm.begin(), perm.end(), [&](int p, int q) { return bkey[p] < bkey[q]; });
+  const std::vector<int> perm = counting_order(nuv, nb1 * nb2, [&](int j) { return bidx[j]; });
   // spreading work items: <= 128 consecutive points of one bin
   std::vector<int> items;
   for (int j = 0; j < nuv;) {
@@ -884,10 +900,7 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
   if (kind != PK_MODEL && d.ndata > 1) {
     auto reorder = [&](int e0, int ne, int s0, int nref) {
       if (ne < 2) return;
-      std::vector<int> ord(ne);
-      std::iota(ord.begin(), ord.end(), 0);
-      std::stable_sort(ord.begin(), ord.end(),
-                       [&](int p, int q) { return didx[s0 + nref * p] < didx[s0 + nref * q]; });
+      const std::vector<int> ord = counting_order(ne, nuv, [&](int p) { return didx[s0 + nref * p]; });
       std::vector<R> r0(ne), r1(ne), r2(ne);
       std::vector<int> ix((size_t)ne * nref);
       std::vector<signed char> sg((size_t)ne * nref);
@@ -995,15 +1008,15 @@ int pack_problem(const smili_imaging_args& a, int kind, int niter, int nonneg, i
     d.o_wy = ar.take(sizeof(R) * (size_t)N * m);
   }
   // ---- blobs ----
-  if (!frame) hp.put(d.o_x0, std::vector<double>(x0, x0 + N));
+  if (!frame) hp.put(d.o_x0, x0, (size_t)N);
   hp.put(d.o_xidx, xi);
   hp.put(d.o_yidx, yi);
   hp.put(d.o_inv, inv);
-  if (d.has_l1) hp.put(d.o_l1w, std::vector<double>(a.l1_wgt, a.l1_wgt + N));
-  if (d.has_tv) hp.put(d.o_tvw, std::vector<double>(a.tv_wgt, a.tv_wgt + N));
-  if (d.has_tsv) hp.put(d.o_tsvw, std::vector<double>(a.tsv_wgt, a.tsv_wgt + N));
-  if (d.has_kl) hp.put(d.o_klw, std::vector<double>(a.kl_wgt, a.kl_wgt + N));
-  if (d.has_gs) hp.put(d.o_gsw, std::vector<double>(a.gs_wgt, a.gs_wgt + N));
+  if (d.has_l1) hp.put(d.o_l1w, a.l1_wgt, (size_t)N);
+  if (d.has_tv) hp.put(d.o_tvw, a.tv_wgt, (size_t)N);
+  if (d.has_tsv) hp.put(d.o_tsvw, a.tsv_wgt, (size_t)N);
+  if (d.has_kl) hp.put(d.o_klw, a.kl_wgt, (size_t)N);
+  if (d.has_gs) hp.put(d.o_gsw, a.gs_wgt, (size_t)N);
   set_uniform_weights(d, a, N);
   hp.put(d.o_dc1, dc1);
   hp.put(d.o_dc2, dc2);
@@ -1531,8 +1544,8 @@ int pack_movie(const smili_imaging3d_args& a, int kind, int niter, int nonneg, i
   // blobs: movie vectors, then every frame's arrays and the frame descriptors
   hp.put(d.o_x0, std::vector<double>(xsrc, xsrc + n));
   hp.put(d.o_lcf, std::vector<double>(a.lc_tgtfd, a.lc_tgtfd + Nz));
-  if (d.has_rt) hp.put(d.o_rtw, std::vector<double>(a.rt_wgt, a.rt_wgt + N));
-  if (d.has_ri) hp.put(d.o_riw, std::vector<double>(a.ri_wgt, a.ri_wgt + N));
+  if (d.has_rt) hp.put(d.o_rtw, a.rt_wgt, (size_t)N);
+  if (d.has_ri) hp.put(d.o_riw, a.ri_wgt, (size_t)N);
   std::vector<ProbDesc> fdesc(Nz);
   for (int z = 0; z < Nz; ++z) {
     fdesc[z] = fh[z].d;
