@@ -60,9 +60,9 @@ sys.path.insert(0, ROOT)
 # this workload at the benchmark's concurrency (74 resident groups of 4
 # CTAs of 512 threads): one ncu capture of ``bench.py --case traffic`` (74
 # problems, 20 iterations) measured dram__bytes_read.sum +
-# dram__bytes_write.sum = 78.10 + 33.07 GB over 2261 evaluations.  The
+# dram__bytes_write.sum = 70.02 + 31.74 GB over 2261 evaluations.  The
 # traffic of a step scales with its evaluation count.
-DRAM_BYTES_PER_EVAL_FP32 = (78.10e9 + 33.07e9) / 2261
+DRAM_BYTES_PER_EVAL_FP32 = (70.02e9 + 31.74e9) / 2261
 
 METRIC = "imaging solves/s at 256²/1e5 vis, FP32+batched+warm-start vs plain, equal final χ²"
 WORKLOAD = ("256x256 / 97 200 uv points (amp 5% + cp + lca), l1/TV/MEM = 1/1/0.1, L-BFGS-B m=5, "
