@@ -650,7 +650,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=296)
+    ap.add_argument("--batch", type=int, default=444)
     ap.add_argument("--seeds", type=int, default=16)
     ap.add_argument("--niter", type=int, default=1000)
     ap.add_argument("--ref-iters", type=int, default=60)
