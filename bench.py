@@ -113,6 +113,20 @@ def fg_bytes(kw, s=4):
             + ncp * (2 * s + 12) + nca * (2 * s + 16) + s * npix * nreg)
 
 
+def task_histogram(codes):
+    """How solves ended, from their L-BFGS-B task codes: reached the target
+    cost, converged (factr / pgtol test), abnormal line-search end, iteration
+    limit, error (a device wait timed out), other."""
+    from smili_b200 import _lib
+    names = {_lib.TASK_TARGET: "target", _lib.TASK_CONV: "converged", _lib.TASK_ABNORMAL: "abnormal",
+             _lib.TASK_STOP: "iteration_limit", _lib.TASK_ERROR: "error"}
+    out = {v: 0 for v in names.values()}
+    for c in codes:
+        k = names.get(int(c), "other")
+        out[k] = out.get(k, 0) + 1
+    return out
+
+
 def lb_bytes_per_iteration(kw, m=5):
     """Compulsory FP64 traffic of one L-BFGS-B iteration (lbfgsb.f v3.0):
     the limited-memory matrices S and Y (2 m n doubles) read by the Cauchy
@@ -722,16 +736,19 @@ def main():
     targets = plain_cost * (1.0 + args.target_rtol)
 
     def quality(b, n, seeds):
-        """Per-solve final cost / plain final cost, target hits, NRMSE."""
-        ratio, hit, err, its = [], 0, [], []
+        """Per-solve final cost / plain final cost, target hits, NRMSE, and
+        how the solves ended (L-BFGS-B task codes: reached the target,
+        converged by factr / pgtol, abnormal line-search end, iteration limit)."""
+        ratio, hit, err, its, codes = [], 0, [], [], []
         for p in range(n):
             x, t, _, i = b.fetch(p)
             k = seeds[p]
             ratio.append(t["cost"] / plain_cost[k])
             hit += i["task"] == _lib.TASK_TARGET
+            codes.append(i["task"])
             err.append(nrmse(kws[k], x, truths[k]))
             its.append(i["niter"])
-        return {"reached_target": int(hit), "solves": n,
+        return {"reached_target": int(hit), "solves": n, "task_codes": task_histogram(codes),
                 "final_cost_over_plain_median": float(np.median(ratio)),
                 "final_cost_over_plain_p10_p90": [float(np.percentile(ratio, 10)),
                                                   float(np.percentile(ratio, 90))],

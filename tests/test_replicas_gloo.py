@@ -56,3 +56,16 @@ def test_one_process_is_the_identity():
     import bench
     assert bench.max_over_ranks(None, 3.0, 4.0, "cpu") == (3.0, 4.0)
     assert bench.job_values(1, 10, 5, 2000.0, 4.0) == (5.0, 2.5, 2.5)
+
+
+def test_task_histogram_names_every_code():
+    """The bench's report of how solves ended: one count per L-BFGS-B task
+    code, unknown codes under "other"."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from smili_b200 import _lib
+    h = bench.task_histogram([_lib.TASK_TARGET, _lib.TASK_TARGET, _lib.TASK_STOP, _lib.TASK_CONV,
+                              _lib.TASK_ABNORMAL, _lib.TASK_ERROR, 99])
+    assert h == {"target": 2, "converged": 1, "abnormal": 1, "iteration_limit": 1, "error": 1, "other": 1}
+    assert bench.task_histogram([]) == {"target": 0, "converged": 0, "abnormal": 0, "iteration_limit": 0,
+                                        "error": 0}
