@@ -1221,8 +1221,8 @@ int finish_batch(smili_batch* b, std::vector<HostProb>& hps, int maxn, const smi
   }
   // launch geometry: co-resident CTAs split into groups
   // FFT/spread staging (SMILI_DYN_CPX complex values) and the Cauchy scan's
-  // batch buffers share the dynamic region: 96 KB in FP64 (two CTAs per SM),
-  // 48 KB in FP32 (three CTAs per SM)
+  // batch buffers share the dynamic region: 96 KB in FP64 (two 256-thread
+  // CTAs per SM), 54 KB in FP32 (two 512-thread CTAs per SM)
   b->dyn_bytes = dyn_smem_bytes<R>();
   const void* fn = (const void*)smili_batch_kernel<R>;
   auto cleanup = [&](int rc) {
